@@ -1,0 +1,144 @@
+/* spect_gpu.h -- C ABI of libspectgpu.so, the B200 (sm_100a) SPECT projector.
+ *
+ * Drop-in boundary for the hot path of SPECTrecon.jl: the bodies of
+ * SPECTplan / project! / backproject! / mlem! / osem! become calls into this
+ * library (Julia `ccall`, Python `ctypes`).  Plain pointers and sizes only.
+ *
+ * Array layout is the reference's Julia column-major layout, unchanged:
+ *   image [nx,ny,nz]        -> C row-major float[nz][ny][nx]
+ *   mumap [nx,ny,nz]        -> float[nz][ny][nx]
+ *   views [nx,nz,nview]     -> float[nview][nz][nx]
+ *   psfs  [px,pz,ny,nview]  -> float[nview][ny][pz][px]
+ * View indices are 0-based here (the Julia shim subtracts 1).
+ *
+ * Every entry point returns an int status (SPECT_OK == 0); the message of the
+ * last failure on the calling thread is spect_last_error().  The messages of
+ * the reference's own throws are kept verbatim (see the status list).
+ *
+ * Pointer kinds: functions named *_host take host arrays and are synchronous
+ * (they copy in, compute, copy out).  The others take device pointers and
+ * enqueue on `stream` (a cudaStream_t, NULL = legacy default stream); they
+ * return as soon as the work is queued.
+ *
+ * Threading: calls on one plan are serialised on the plan's work buffers, so
+ * use one plan per host thread (the reference plan is not re-entrant either,
+ * src/spectplan.jl:95-112).  Distinct plans may run concurrently.
+ */
+#ifndef SPECT_GPU_H
+#define SPECT_GPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; messages mirror the reference's throws */
+enum {
+  SPECT_OK = 0,
+  SPECT_ERR_NX_NE_NY = 1,      /* "nx != ny"            src/spectplan.jl:76 (98 in file) */
+  SPECT_ERR_NX_ODD = 2,        /* "nx odd"              src/spectplan.jl:77 (99) */
+  SPECT_ERR_PSF_NOT_ODD = 3,   /* "non-odd size psfs"   src/spectplan.jl:82 (104) */
+  SPECT_ERR_PSF_ASYM = 4,      /* "asym. psf"           src/spectplan.jl:83-84 (105-106) */
+  SPECT_ERR_INTERP = 5,        /* "bad interpmeth"      src/spectplan.jl:87 (109) */
+  SPECT_ERR_NTHREAD = 6,       /* "bad nthread"         src/spectplan.jl:90 (112) */
+  SPECT_ERR_MODE = 7,          /* "bad mode"            src/spectplan.jl:93 (115) */
+  SPECT_ERR_DIM = 8,           /* DimensionMismatch     src/project.jl:204-205, src/ml-os-em.jl:25-26 */
+  SPECT_ERR_BACKGROUND = 9,    /* "need background > 0" src/ml-os-em.jl:30,106 (324,400) */
+  SPECT_ERR_NBLOCKS = 10,      /* "nview must be divisible by nblocks!" src/ml-os-em.jl:73 (367) */
+  SPECT_ERR_INDEX = 11,        /* view index out of 0..nview-1 (Julia BoundsError) */
+  SPECT_ERR_ARG = 12,          /* null pointer / non-positive size */
+  SPECT_ERR_UNSUPPORTED = 13,  /* size beyond this build's kernel limits */
+  SPECT_ERR_CUDA = 14,         /* CUDA runtime error (message has the detail) */
+  SPECT_ERR_OOM = 15,          /* device allocation failed / memory budget */
+  SPECT_ERR_TIMEOUT = 16,      /* a bounded device wait gave up */
+  SPECT_ERR_BUSY = 17          /* resource in use (serving slot table full) */
+};
+
+/* interpolation method of SPECTplan(...; interpmeth) */
+enum { SPECT_INTERP_ONE = 1, SPECT_INTERP_TWO = 2 };
+/* SPECTplan(...; mode): accepted and validated, no effect on the GPU */
+enum { SPECT_MODE_FAST = 0, SPECT_MODE_MEM = 1 };
+
+typedef struct spect_plan_s* spect_plan_t;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* spect_last_error(void);
+
+/* Library/device information: fills sm count, total device memory (bytes). */
+int spect_device_info(int* sm_count, size_t* total_mem);
+
+/* SPECTplan(mumap, psfs, dy; T, viewangle, interpmeth, nthread, mode)
+ * (src/spectplan.jl:58-137; 80-159 in file).  mumap and psfs are HOST arrays;
+ * they are validated exactly as the reference does (nx == ny, nx even, px/pz
+ * odd, every psfs[:,:,y,v] point-symmetric, interpmeth, nthread == nthreads,
+ * mode), uploaded, and the PSF spectra are precomputed on the device.  Unlike
+ * the reference plan, later edits of the host mumap/psfs are not seen.
+ * viewangle may be NULL for the default (0:nview-1)/nview*2pi rounded to
+ * Float32; otherwise nview angles in radians.  `nthreads` is the caller's
+ * thread count (Julia: Threads.nthreads()). */
+int spect_plan_create(spect_plan_t* plan, int nx, int ny, int nz, int px, int pz, int nview,
+                      const float* mumap, const float* psfs, float dy, const float* viewangle,
+                      int interpmeth, int mode, int nthread, int nthreads);
+int spect_plan_destroy(spect_plan_t plan);
+
+/* Sizes and device memory held by the plan: out[0..7] = nx, ny, nz, px, pz,
+ * nview, interpmeth, number of distinct PSF spectrum sets; *bytes = device
+ * bytes held by the plan. */
+int spect_plan_info(spect_plan_t plan, int out[8], size_t* bytes);
+
+/* project!(views, image, plan; index) (src/project.jl:143-163).
+ * views[nindex][nz][nx] = P_{index[i]} image; index NULL = all views in order
+ * (nindex must then be nview).  Device pointers, enqueued on stream. */
+int spect_project(spect_plan_t plan, float* views, const float* image, const int32_t* index, int nindex,
+                  void* stream);
+/* Same with host arrays; synchronous. */
+int spect_project_host(spect_plan_t plan, float* views, const float* image, const int32_t* index,
+                       int nindex);
+
+/* backproject!(image, views, plan; index) (src/backproject.jl:132-162; 340-370
+ * in file).  image = sum_i P_{index[i]}' views[i]; image need not be zeroed. */
+int spect_backproject(spect_plan_t plan, float* image, const float* views, const int32_t* index,
+                      int nindex, void* stream);
+int spect_backproject_host(spect_plan_t plan, float* image, const float* views, const int32_t* index,
+                           int nindex);
+
+/* mlem!(out, x0, ynoisy, background, A; niter) (src/ml-os-em.jl:21-49;
+ * 315-343 in file) with A the plan's full projector.  Device pointers; the
+ * EM ratio is fused into the forward reduction and the multiplicative update
+ * into the back-projection's last stage. */
+int spect_mlem(spect_plan_t plan, float* out, const float* x0, const float* ynoisy,
+               const float* background, int niter, void* stream);
+int spect_mlem_host(spect_plan_t plan, float* out, const float* x0, const float* ynoisy,
+                    const float* background, int niter);
+
+/* osem!(out, x0, ynoisy, background, Ablock(plan, nblocks); niter)
+ * (src/ml-os-em.jl:70-131; 364-425 in file): subsets nb:nblocks:nview. */
+int spect_osem(spect_plan_t plan, float* out, const float* x0, const float* ynoisy,
+               const float* background, int nblocks, int niter, void* stream);
+int spect_osem_host(spect_plan_t plan, float* out, const float* x0, const float* ynoisy,
+                    const float* background, int nblocks, int niter);
+
+/* One fused OS-EM subset update on device buffers (the loop body of
+ * src/ml-os-em.jl:123-127; 417-421 in file):
+ *   x .*= A_s' (y_s ./ (A_s x + b_s)) ./ asum
+ * y and background are the FULL [nview][nz][nx] arrays; the subset is
+ * index[0..nindex).  asum is A_s' 1 with zeros replaced by +Inf. */
+int spect_em_subset_update(spect_plan_t plan, float* x, const float* ynoisy, const float* background,
+                           const float* asum, const int32_t* index, int nindex, void* stream);
+
+/* asum = A_s' 1 with zeros replaced by +Inf (src/ml-os-em.jl:111-114). */
+int spect_subset_sensitivity(spect_plan_t plan, float* asum, const int32_t* index, int nindex,
+                             void* stream);
+
+/* psf_gauss(; ny, px, pz, fwhm_x, fwhm_z) (src/psf-gauss.jl:24-55): host
+ * generator of depth-dependent Gaussian PSFs into psf[ny][pz][px] (Julia
+ * psf[px,pz,ny]).  fwhm_x/fwhm_z hold ny values (fwhm_z NULL = fwhm_x). */
+int spect_psf_gauss(float* psf, int ny, int px, int pz, const double* fwhm_x, const double* fwhm_z);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPECT_GPU_H */

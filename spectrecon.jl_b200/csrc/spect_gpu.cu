@@ -1,0 +1,750 @@
+// spect_gpu.cu -- C ABI of the B200 SPECT projector (declared in include/spect_gpu.h).
+//
+// Host side of the drop-in boundary: SPECTplan construction and validation
+// (src/spectplan.jl:58-137), project!/backproject! over a view index list
+// (src/project.jl:143-163, src/backproject.jl:132-162), ML-EM / OS-EM with the
+// EM ratio and multiplicative update fused into the projector's last stages
+// (src/ml-os-em.jl:21-131), and psf_gauss (src/psf-gauss.jl:24-55).
+//
+// Device memory layout (HBM), all float32 unless noted:
+//   mumap   [nz][ny][nx]                 uploaded once per plan
+//   H       [nset][ny][Hz][Npx]          real PSF spectra, one set per distinct
+//                                        psfs[:,:,:,v] (views with identical
+//                                        PSF stacks share a set)
+//   P / T   [gmax][ny][nz][nx]           rotated+attenuated planes (forward) /
+//                                        adjoint-convolved planes (adjoint) of
+//                                        one group of views
+//   part    [gmax][nchunk][nz][nx]       per depth-chunk partial views
+//   Vhat    [gmax][Hz][Npx] complex      spectra of the views (adjoint)
+//   imgpart [nsplit][nz][ny][nx]         per view-split partial images
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/spect_gpu.h"
+#include "spect_kernels.cuh"
+
+using namespace spect;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                                  \
+  do {                                                                                                  \
+    cudaError_t e_ = (expr);                                                                            \
+    if (e_ != cudaSuccess) {                                                                            \
+      return fail(e_ == cudaErrorMemoryAllocation ? SPECT_ERR_OOM : SPECT_ERR_CUDA,                     \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                                  \
+    }                                                                                                   \
+  } while (0)
+
+#define STATUS_TRY(expr)       \
+  do {                         \
+    int st_ = (expr);          \
+    if (st_ != SPECT_OK) return st_; \
+  } while (0)
+
+inline int power2(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+inline int ilog2(int x) {
+  int l = 0;
+  while ((1 << l) < x) ++l;
+  return l;
+}
+inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+constexpr double kTwoPi = 6.283185307179586;
+
+}  // namespace
+
+struct spect_plan_s {
+  int nx, ny, nz, px, pz, nview, interp, mode, nthread;
+  float dy;
+  Geom g;
+  int device = 0, sm_count = 148;
+  size_t max_smem = 232448;
+  int nset = 0;
+  std::vector<int> view_set;
+  std::vector<float> angles;
+  size_t N = 0, nxz = 0;
+  // device
+  float* d_mumap = nullptr;
+  float* d_H = nullptr;
+  float4* d_rot = nullptr;
+  int* d_viewset = nullptr;
+  float2* d_tw = nullptr;
+  int* d_all = nullptr;  // 0..nview-1
+  int* d_idx = nullptr;  // per-call index staging [nview]
+  // work scratch for one group of views
+  int gmax = 1, nchunk_max = 16;
+  float* d_P = nullptr;
+  float* d_part = nullptr;
+  float2* d_Vhat = nullptr;
+  float* d_imgpart = nullptr;
+  float2* d_gB = nullptr;
+  float* d_gacc = nullptr;
+  float* d_gscr_adj = nullptr;
+  // EM scratch (lazily allocated)
+  float* d_views_tmp = nullptr;  // [nview][nz][nx]
+  float* d_ones = nullptr;       // [nview][nz][nx]
+  float* d_asum = nullptr;       // [nblocks][N]
+  int asum_blocks = 0;
+  int* d_flag = nullptr;
+  // host-call staging (lazily allocated)
+  float* d_io_img = nullptr;   // [2][N]
+  float* d_io_views = nullptr; // [3][nview][nz][nx]
+  // launch configuration
+  int conv_grid = 148, conv_bsmem = 1, conv_asmem = 1;
+  size_t conv_smem = 0;
+  int rotf_vpb = 1, rotf_smem_ok = 1;
+  size_t rotf_smem = 0;
+  int rota_smem_ok = 1, nsplit_adj = 1;
+  size_t rota_smem = 0;
+  size_t bytes = 0;
+  std::mutex mu;
+};
+
+namespace {
+
+template <class T>
+int dalloc(spect_plan_s* p, T** ptr, size_t count) {
+  size_t b = sizeof(T) * std::max<size_t>(count, 1);
+  cudaError_t e = cudaMalloc((void**)ptr, b);
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? SPECT_ERR_OOM : SPECT_ERR_CUDA,
+                std::string("cudaMalloc(") + std::to_string(b) + " bytes): " + cudaGetErrorString(e));
+  }
+  p->bytes += b;
+  return SPECT_OK;
+}
+
+void free_plan(spect_plan_s* p) {
+  void* ptrs[] = {p->d_mumap, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
+                  p->d_idx,   p->d_P,     p->d_part,     p->d_Vhat,      p->d_imgpart,    p->d_gB,
+                  p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag,
+                  p->d_io_img, p->d_io_views};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete p;
+}
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  return SPECT_OK;
+}
+
+// Launch configuration that depends only on the plan's sizes.
+int configure(spect_plan_s* p) {
+  int dev;
+  CUDA_TRY(cudaGetDevice(&dev));
+  p->device = dev;
+  CUDA_TRY(cudaDeviceGetAttribute(&p->sm_count, cudaDevAttrMultiProcessorCount, dev));
+  int optin = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  p->max_smem = (size_t)optin;
+  const Geom& g = p->g;
+  // ---- convolution kernels
+  const int maxN = std::max(g.Npx, g.Npz);
+  size_t base = sizeof(float2) * (SPECT_TW_N + (size_t)kConvWarps * maxN);
+  size_t Bb = sizeof(float2) * (size_t)g.nx * g.Hz;
+  size_t Ab = sizeof(float) * (size_t)g.nz * (g.nx + 2);
+  if (base + Bb + Ab <= p->max_smem) {
+    p->conv_bsmem = 1;
+    p->conv_asmem = 1;
+    p->conv_smem = base + Bb + Ab;
+  } else if (base + Bb <= p->max_smem) {
+    p->conv_bsmem = 1;
+    p->conv_asmem = 0;
+    p->conv_smem = base + Bb;
+  } else {
+    p->conv_bsmem = 0;
+    p->conv_asmem = (base + Ab <= p->max_smem) ? 1 : 0;
+    p->conv_smem = base + (p->conv_asmem ? Ab : 0);
+  }
+  const void* convk[] = {(const void*)k_conv_fwd, (const void*)k_conv_adj, (const void*)k_vspec};
+  int occ = 8;
+  for (const void* k : convk) {
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->conv_smem));
+    int o = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, kConvThreads, p->conv_smem));
+    occ = std::min(occ, std::max(o, 1));
+  }
+  p->conv_grid = p->sm_count * occ;
+  if (!p->conv_bsmem) STATUS_TRY(dalloc(p, &p->d_gB, (size_t)g.nx * g.Hz * p->conv_grid));
+  if (!p->conv_asmem) STATUS_TRY(dalloc(p, &p->d_gacc, (size_t)g.nz * (g.nx + 2) * p->conv_grid));
+  // ---- forward rotation
+  p->rotf_vpb = std::max(1, std::min(8, 512 / g.nx));
+  size_t slice = (size_t)g.nx * g.ny;
+  p->rotf_smem = 2 * slice * sizeof(float);
+  p->rotf_smem_ok = p->rotf_smem <= p->max_smem;
+  if (p->rotf_smem_ok)
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)p->rotf_smem));
+  // ---- adjoint rotation
+  int nseg = std::max(1, kRotAdjThreads / g.nx);
+  p->rota_smem = (2 * slice + (size_t)nseg * g.nx) * sizeof(float);
+  p->rota_smem_ok = p->rota_smem <= p->max_smem;
+  p->nsplit_adj = std::max(1, std::min(8, cdiv(2 * p->sm_count, g.nz)));
+  if (p->rota_smem_ok) {
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)p->rota_smem));
+  } else {
+    size_t per = 2 * slice + (size_t)nseg * g.nx;
+    STATUS_TRY(dalloc(p, &p->d_gscr_adj, per * g.nz * p->nsplit_adj));
+  }
+  return SPECT_OK;
+}
+
+// chunking of the depth planes for a call with nv views
+void chunking(const spect_plan_s* p, int nv, int* chunkY, int* nchunks) {
+  int target = 4 * p->conv_grid;
+  int nc = std::max(1, std::min(std::min(p->nchunk_max, p->ny), cdiv(target, std::max(nv, 1))));
+  int cy = cdiv(p->ny, nc);
+  *chunkY = cy;
+  *nchunks = cdiv(p->ny, cy);
+}
+
+ConvArgs conv_args(const spect_plan_s* p) {
+  ConvArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = p->g;
+  a.H = p->d_H;
+  a.viewset = p->d_viewset;
+  a.gB = p->d_gB;
+  a.gacc = p->d_gacc;
+  a.tw = p->d_tw;
+  a.bsmem = p->conv_bsmem;
+  a.asmem = p->conv_asmem;
+  return a;
+}
+
+// forward projection of nidx views (device index list vidx) into views;
+// with y/bg non-null the output is the EM ratio y/(A x + bg).
+int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, int nidx, cudaStream_t st,
+            const float* y, const float* bg) {
+  const Geom& g = p->g;
+  if (p->interp != SPECT_INTERP_TWO) return fail(SPECT_ERR_UNSUPPORTED, "interpmeth :one is not available on the GPU path");
+  for (int g0 = 0; g0 < nidx; g0 += p->gmax) {
+    const int nv = std::min(p->gmax, nidx - g0);
+    const int* vi = vidx + g0;
+    // rotation + attenuation -> P
+    int vpb = p->rotf_vpb;
+    int nsplit = std::max(1, std::min(cdiv(2 * p->sm_count, g.nz), cdiv(nv, vpb)));
+    dim3 grid(g.nz, nsplit);
+    if (p->rotf_smem_ok)
+      k_rot_fwd<true><<<grid, g.nx * vpb, p->rotf_smem, st>>>(g, image, p->d_mumap, p->d_rot, vi, nv, p->d_P);
+    else
+      k_rot_fwd<false><<<grid, g.nx * vpb, 0, st>>>(g, image, p->d_mumap, p->d_rot, vi, nv, p->d_P);
+    STATUS_TRY(check_launch("k_rot_fwd"));
+    // FFT convolution + depth sum -> part
+    ConvArgs a = conv_args(p);
+    int cy, nc;
+    chunking(p, nv, &cy, &nc);
+    a.P = p->d_P;
+    a.vidx = vi;
+    a.nv = nv;
+    a.chunkY = cy;
+    a.nchunks = nc;
+    a.part = p->d_part;
+    int gridc = std::min(p->conv_grid, nv * nc);
+    k_conv_fwd<<<gridc, kConvThreads, p->conv_smem, st>>>(a);
+    STATUS_TRY(check_launch("k_conv_fwd"));
+    // chunk sum (+ EM ratio) -> views
+    size_t n = (size_t)nv * p->nxz;
+    int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16);
+    k_reduce_views<<<rb, 256, 0, st>>>(p->d_part, nv, nc, (int)p->nxz, views + (size_t)g0 * p->nxz, y, bg, vi);
+    STATUS_TRY(check_launch("k_reduce_views"));
+  }
+  return SPECT_OK;
+}
+
+// back-projection of nidx views.  mode 0: image = A' views; mode 1: image =
+// A' views with zeros -> Inf (EM sensitivity); mode 2: image .*= (A' views) ./ asum
+int backward(spect_plan_s* p, float* image, const float* views, const int* vidx, int nidx, cudaStream_t st,
+             int mode, const float* asum) {
+  const Geom& g = p->g;
+  if (p->interp != SPECT_INTERP_TWO) return fail(SPECT_ERR_UNSUPPORTED, "interpmeth :one is not available on the GPU path");
+  const int nsplit = p->nsplit_adj;
+  if (nidx == 0) {
+    CUDA_TRY(cudaMemsetAsync(p->d_imgpart, 0, sizeof(float) * p->N * nsplit, st));
+  }
+  for (int g0 = 0; g0 < nidx; g0 += p->gmax) {
+    const int nv = std::min(p->gmax, nidx - g0);
+    const int* vi = vidx + g0;
+    ConvArgs a = conv_args(p);
+    a.views = views + (size_t)g0 * p->nxz;
+    a.VhatOut = p->d_Vhat;
+    a.nv = nv;
+    a.vidx = vi;
+    k_vspec<<<std::min(p->conv_grid, nv), kConvThreads, p->conv_smem, st>>>(a);
+    STATUS_TRY(check_launch("k_vspec"));
+    int cy, nc;
+    chunking(p, nv, &cy, &nc);
+    a.Vhat = p->d_Vhat;
+    a.T = p->d_P;
+    a.chunkY = cy;
+    a.nchunks = nc;
+    k_conv_adj<<<std::min(p->conv_grid, nv * nc), kConvThreads, p->conv_smem, st>>>(a);
+    STATUS_TRY(check_launch("k_conv_adj"));
+    dim3 grid(g.nz, nsplit);
+    k_rot_adj<<<grid, kRotAdjThreads, p->rota_smem_ok ? p->rota_smem : 0, st>>>(
+        g, p->d_P, p->d_mumap, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok, p->d_gscr_adj);
+    STATUS_TRY(check_launch("k_rot_adj"));
+  }
+  int rb = (int)std::min<size_t>((p->N + 255) / 256, (size_t)p->sm_count * 16);
+  k_reduce_image<<<rb, 256, 0, st>>>(p->d_imgpart, nsplit, p->N, image, asum, mode == 2 ? 1 : 0, mode == 1 ? 1 : 0);
+  STATUS_TRY(check_launch("k_reduce_image"));
+  return SPECT_OK;
+}
+
+int stage_index(spect_plan_s* p, const int32_t* index, int nindex, cudaStream_t st, const int** dev) {
+  if (!index) {
+    if (nindex != p->nview) return fail(SPECT_ERR_DIM, "DimensionMismatch: index=NULL needs nindex == nview");
+    *dev = p->d_all;
+    return SPECT_OK;
+  }
+  if (nindex < 0 || nindex > p->nview)
+    return fail(SPECT_ERR_DIM, "DimensionMismatch: nindex must be in 0..nview");
+  for (int i = 0; i < nindex; ++i)
+    if (index[i] < 0 || index[i] >= p->nview)
+      return fail(SPECT_ERR_INDEX, "BoundsError: view index " + std::to_string(index[i]) + " not in 0.." +
+                                       std::to_string(p->nview - 1));
+  CUDA_TRY(cudaMemcpyAsync(p->d_idx, index, sizeof(int) * nindex, cudaMemcpyHostToDevice, st));
+  *dev = p->d_idx;
+  return SPECT_OK;
+}
+
+int ensure_em(spect_plan_s* p, int nblocks) {
+  size_t V = (size_t)p->nview * p->nxz;
+  if (!p->d_views_tmp) STATUS_TRY(dalloc(p, &p->d_views_tmp, V));
+  if (!p->d_ones) {
+    STATUS_TRY(dalloc(p, &p->d_ones, V));
+    std::vector<float> h(V, 1.0f);
+    CUDA_TRY(cudaMemcpy(p->d_ones, h.data(), sizeof(float) * V, cudaMemcpyHostToDevice));
+  }
+  if (!p->d_flag) STATUS_TRY(dalloc(p, &p->d_flag, 1));
+  if (p->asum_blocks < nblocks) {
+    if (p->d_asum) {
+      cudaFree(p->d_asum);
+      p->bytes -= sizeof(float) * p->N * p->asum_blocks;
+    }
+    p->d_asum = nullptr;
+    STATUS_TRY(dalloc(p, &p->d_asum, p->N * nblocks));
+    p->asum_blocks = nblocks;
+  }
+  return SPECT_OK;
+}
+
+__global__ void k_all_positive(const float* __restrict__ b, size_t n, int* flag) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    if (!(b[k] > 0.f)) *flag = 1;
+}
+
+int check_background(spect_plan_s* p, const float* bg, cudaStream_t st) {
+  size_t V = (size_t)p->nview * p->nxz;
+  CUDA_TRY(cudaMemsetAsync(p->d_flag, 0, sizeof(int), st));
+  k_all_positive<<<std::max(1, std::min(cdiv(V, 256), p->sm_count * 8)), 256, 0, st>>>(bg, V, p->d_flag);
+  STATUS_TRY(check_launch("k_all_positive"));
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, p->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) return fail(SPECT_ERR_BACKGROUND, "need background > 0");
+  return SPECT_OK;
+}
+
+// OS-EM on device buffers (mlem = one block)
+int run_osem(spect_plan_s* p, float* out, const float* x0, const float* y, const float* bg, int nblocks, int niter,
+             cudaStream_t st) {
+  if (nblocks < 1 || p->nview % nblocks != 0) return fail(SPECT_ERR_NBLOCKS, "nview must be divisible by nblocks!");
+  if (niter < 0) return fail(SPECT_ERR_ARG, "niter must be >= 0");
+  STATUS_TRY(ensure_em(p, nblocks));
+  STATUS_TRY(check_background(p, bg, st));
+  const int nsub = p->nview / nblocks;
+  std::vector<int> idx(p->nview);
+  for (int b = 0; b < nblocks; ++b)
+    for (int s = 0; s < nsub; ++s) idx[(size_t)b * nsub + s] = b + s * nblocks;
+  CUDA_TRY(cudaMemcpyAsync(p->d_idx, idx.data(), sizeof(int) * p->nview, cudaMemcpyHostToDevice, st));
+  for (int b = 0; b < nblocks; ++b)
+    STATUS_TRY(backward(p, p->d_asum + (size_t)b * p->N, p->d_ones, p->d_idx + (size_t)b * nsub, nsub, st, 1,
+                        nullptr));
+  if (out != x0) CUDA_TRY(cudaMemcpyAsync(out, x0, sizeof(float) * p->N, cudaMemcpyDeviceToDevice, st));
+  for (int it = 0; it < niter; ++it)
+    for (int b = 0; b < nblocks; ++b) {
+      const int* vi = p->d_idx + (size_t)b * nsub;
+      STATUS_TRY(forward(p, p->d_views_tmp, out, vi, nsub, st, y, bg));
+      STATUS_TRY(backward(p, out, p->d_views_tmp, vi, nsub, st, 2, p->d_asum + (size_t)b * p->N));
+    }
+  return SPECT_OK;
+}
+
+int ensure_io(spect_plan_s* p) {
+  if (!p->d_io_img) STATUS_TRY(dalloc(p, &p->d_io_img, 2 * p->N));
+  if (!p->d_io_views) STATUS_TRY(dalloc(p, &p->d_io_views, 3 * (size_t)p->nview * p->nxz));
+  return SPECT_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+const char* spect_last_error(void) { return g_err.c_str(); }
+
+int spect_device_info(int* sm_count, size_t* total_mem) {
+  int dev;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (sm_count) CUDA_TRY(cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev));
+  if (total_mem) {
+    size_t f, t;
+    CUDA_TRY(cudaMemGetInfo(&f, &t));
+    *total_mem = t;
+  }
+  return SPECT_OK;
+}
+
+int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview, const float* mumap,
+                      const float* psfs, float dy, const float* viewangle, int interpmeth, int mode, int nthread,
+                      int nthreads) {
+  if (!out || !mumap || !psfs) return fail(SPECT_ERR_ARG, "null pointer argument");
+  *out = nullptr;
+  if (nx <= 0 || ny <= 0 || nz <= 0 || px <= 0 || pz <= 0 || nview <= 0)
+    return fail(SPECT_ERR_ARG, "sizes must be positive");
+  // validation in the reference's order (src/spectplan.jl:76-93)
+  if (nx != ny) return fail(SPECT_ERR_NX_NE_NY, "nx != ny");
+  if ((nx % 2) || (ny % 2)) return fail(SPECT_ERR_NX_ODD, "nx odd");
+  if (!(px % 2) || !(pz % 2)) return fail(SPECT_ERR_PSF_NOT_ODD, "non-odd size psfs");
+  const size_t pp = (size_t)px * pz;
+  for (size_t pl = 0; pl < (size_t)ny * nview; ++pl) {
+    const float* k = psfs + pl * pp;
+    for (size_t i = 0; i < pp; ++i)
+      if (!(k[i] == k[pp - 1 - i])) return fail(SPECT_ERR_PSF_ASYM, "asym. psf");
+  }
+  if (interpmeth != SPECT_INTERP_ONE && interpmeth != SPECT_INTERP_TWO)
+    return fail(SPECT_ERR_INTERP, "bad interpmeth");
+  if (nthread != nthreads) return fail(SPECT_ERR_NTHREAD, "bad nthread");
+  if (mode != SPECT_MODE_FAST && mode != SPECT_MODE_MEM) return fail(SPECT_ERR_MODE, "bad mode");
+  const int Npx = power2(nx + px - 1), Npz = power2(nz + pz - 1);
+  if (Npx > SPECT_TW_N || Npz > SPECT_TW_N || nx > 512)
+    return fail(SPECT_ERR_UNSUPPORTED, "padded plane " + std::to_string(Npx) + "x" + std::to_string(Npz) +
+                                           " exceeds this build's FFT limit of " + std::to_string(SPECT_TW_N));
+
+  spect_plan_s* p = new spect_plan_s;
+  p->nx = nx;
+  p->ny = ny;
+  p->nz = nz;
+  p->px = px;
+  p->pz = pz;
+  p->nview = nview;
+  p->interp = interpmeth;
+  p->mode = mode;
+  p->nthread = nthread;
+  p->dy = dy;
+  p->N = (size_t)nx * ny * nz;
+  p->nxz = (size_t)nx * nz;
+  Geom& g = p->g;
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = nz;
+  g.Npx = Npx;
+  g.Npz = Npz;
+  g.logNpx = ilog2(Npx);
+  g.logNpz = ilog2(Npz);
+  g.Hz = Npz / 2 + 1;
+  g.padup = (Npx - nx + 1) / 2;
+  g.padleft = (Npz - nz + 1) / 2;
+  g.dy = dy;
+  g.c0 = (float)((nx - 1) * 0.5);
+  auto bail = [&](int st) {
+    free_plan(p);
+    return st;
+  };
+  int st = configure(p);
+  if (st != SPECT_OK) return bail(st);
+
+  // angles: default (0:nview-1)/nview * Float32(2pi), element rounded to Float32
+  p->angles.resize(nview);
+  const double t2pi = (double)(float)kTwoPi;
+  for (int v = 0; v < nview; ++v) p->angles[v] = viewangle ? viewangle[v] : (float)((double)v / nview * t2pi);
+  std::vector<float4> rot(nview);
+  for (int v = 0; v < nview; ++v) {
+    double phi = kTwoPi - (double)p->angles[v];
+    bool ident = std::fmod((double)p->angles[v], kTwoPi) == 0.0;
+    rot[v] = make_float4((float)std::cos(phi), (float)std::sin(phi), ident ? 1.f : 0.f, p->angles[v]);
+  }
+  // distinct PSF stacks
+  const size_t stack = (size_t)ny * pp;
+  std::vector<int> uniq;
+  p->view_set.resize(nview);
+  for (int v = 0; v < nview; ++v) {
+    int found = -1;
+    for (size_t u = 0; u < uniq.size(); ++u)
+      if (std::memcmp(psfs + (size_t)uniq[u] * stack, psfs + (size_t)v * stack, sizeof(float) * stack) == 0) {
+        found = (int)u;
+        break;
+      }
+    if (found < 0) {
+      found = (int)uniq.size();
+      uniq.push_back(v);
+    }
+    p->view_set[v] = found;
+  }
+  p->nset = (int)uniq.size();
+
+  // group size: rotated-plane scratch bounded by ~1 GiB
+  const size_t budget = (size_t)1 << 30;
+  p->gmax = (int)std::max<size_t>(1, std::min<size_t>((size_t)nview, budget / (sizeof(float) * p->N)));
+
+  if ((st = dalloc(p, &p->d_mumap, p->N)) || (st = dalloc(p, &p->d_rot, nview)) ||
+      (st = dalloc(p, &p->d_viewset, nview)) || (st = dalloc(p, &p->d_tw, SPECT_TW_N)) ||
+      (st = dalloc(p, &p->d_all, nview)) || (st = dalloc(p, &p->d_idx, nview)) ||
+      (st = dalloc(p, &p->d_H, (size_t)p->nset * ny * g.Hz * Npx)) ||
+      (st = dalloc(p, &p->d_P, (size_t)p->gmax * p->N)) ||
+      (st = dalloc(p, &p->d_part, (size_t)p->gmax * p->nchunk_max * p->nxz)) ||
+      (st = dalloc(p, &p->d_Vhat, (size_t)p->gmax * g.Hz * Npx)) ||
+      (st = dalloc(p, &p->d_imgpart, (size_t)p->nsplit_adj * p->N)))
+    return bail(st);
+
+  std::vector<float2> tw(SPECT_TW_N);
+  for (int m = 0; m < SPECT_TW_N; ++m) {
+    double a = -kTwoPi * m / SPECT_TW_N;
+    tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  std::vector<int> all(nview);
+  for (int v = 0; v < nview; ++v) all[v] = v;
+  auto up = [&](void* d, const void* h, size_t b) -> int {
+    cudaError_t e = cudaMemcpy(d, h, b, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+    return SPECT_OK;
+  };
+  if ((st = up(p->d_mumap, mumap, sizeof(float) * p->N)) || (st = up(p->d_rot, rot.data(), sizeof(float4) * nview)) ||
+      (st = up(p->d_viewset, p->view_set.data(), sizeof(int) * nview)) ||
+      (st = up(p->d_tw, tw.data(), sizeof(float2) * SPECT_TW_N)) ||
+      (st = up(p->d_all, all.data(), sizeof(int) * nview)))
+    return bail(st);
+
+  // PSF spectra, in batches of planes (double precision on the device)
+  {
+    std::vector<double2> wx(Npx), wz(Npz);
+    for (int m = 0; m < Npx; ++m) wx[m] = make_double2(std::cos(-kTwoPi * m / Npx), std::sin(-kTwoPi * m / Npx));
+    for (int m = 0; m < Npz; ++m) wz[m] = make_double2(std::cos(-kTwoPi * m / Npz), std::sin(-kTwoPi * m / Npz));
+    const size_t nplanes = (size_t)p->nset * ny;
+    const size_t per_plane_G = (size_t)pz * Npx * sizeof(double2);
+    const size_t batch = std::max<size_t>(1, std::min(nplanes, ((size_t)256 << 20) / per_plane_G));
+    double2 *d_wx = nullptr, *d_wz = nullptr, *d_G = nullptr;
+    float* d_psf = nullptr;
+    auto cleanup = [&]() {
+      if (d_wx) cudaFree(d_wx);
+      if (d_wz) cudaFree(d_wz);
+      if (d_G) cudaFree(d_G);
+      if (d_psf) cudaFree(d_psf);
+    };
+    cudaError_t e = cudaSuccess;
+    e = cudaMalloc((void**)&d_wx, sizeof(double2) * Npx);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_wz, sizeof(double2) * Npz);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_G, per_plane_G * batch);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_psf, sizeof(float) * pp * batch);
+    if (e == cudaSuccess) e = cudaMemcpy(d_wx, wx.data(), sizeof(double2) * Npx, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_wz, wz.data(), sizeof(double2) * Npz, cudaMemcpyHostToDevice);
+    std::vector<float> hp(pp * batch);
+    for (size_t b0 = 0; e == cudaSuccess && b0 < nplanes; b0 += batch) {
+      size_t nb = std::min(batch, nplanes - b0);
+      for (size_t q = 0; q < nb; ++q) {
+        size_t pl = b0 + q;
+        size_t set = pl / ny, y = pl % ny;
+        std::memcpy(hp.data() + q * pp, psfs + ((size_t)uniq[set] * ny + y) * pp, sizeof(float) * pp);
+      }
+      e = cudaMemcpy(d_psf, hp.data(), sizeof(float) * pp * nb, cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) break;
+      int blocks = std::min(cdiv((long long)nb * pz * Npx, 256), p->sm_count * 32);
+      k_psf_stage1<<<blocks, 256>>>(d_psf, (int)nb, px, pz, Npx, d_wx, d_G);
+      blocks = std::min(cdiv((long long)nb * g.Hz * Npx, 256), p->sm_count * 32);
+      k_psf_stage2<<<blocks, 256>>>(d_G, (int)nb, pz, Npx, Npz, g.Hz, d_wz, p->d_H + b0 * g.Hz * Npx);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    cleanup();
+    if (e != cudaSuccess) {
+      fail(SPECT_ERR_CUDA, std::string("PSF spectra: ") + cudaGetErrorString(e));
+      return bail(SPECT_ERR_CUDA);
+    }
+  }
+  *out = p;
+  return SPECT_OK;
+}
+
+int spect_plan_destroy(spect_plan_t p) {
+  if (!p) return fail(SPECT_ERR_ARG, "null plan");
+  cudaDeviceSynchronize();
+  free_plan(p);
+  return SPECT_OK;
+}
+
+int spect_plan_info(spect_plan_t p, int out[8], size_t* bytes) {
+  if (!p || !out) return fail(SPECT_ERR_ARG, "null pointer argument");
+  int v[8] = {p->nx, p->ny, p->nz, p->px, p->pz, p->nview, p->interp, p->nset};
+  std::memcpy(out, v, sizeof(v));
+  if (bytes) *bytes = p->bytes;
+  return SPECT_OK;
+}
+
+int spect_project(spect_plan_t p, float* views, const float* image, const int32_t* index, int nindex, void* stream) {
+  if (!p || !views || !image) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int* vi;
+  STATUS_TRY(stage_index(p, index, nindex, st, &vi));
+  return forward(p, views, image, vi, nindex, st, nullptr, nullptr);
+}
+
+int spect_project_host(spect_plan_t p, float* views, const float* image, const int32_t* index, int nindex) {
+  if (!p || !views || !image) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  STATUS_TRY(ensure_io(p));
+  cudaStream_t st = 0;
+  const int* vi;
+  STATUS_TRY(stage_index(p, index, nindex, st, &vi));
+  CUDA_TRY(cudaMemcpyAsync(p->d_io_img, image, sizeof(float) * p->N, cudaMemcpyHostToDevice, st));
+  STATUS_TRY(forward(p, p->d_io_views, p->d_io_img, vi, nindex, st, nullptr, nullptr));
+  CUDA_TRY(cudaMemcpyAsync(views, p->d_io_views, sizeof(float) * nindex * p->nxz, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SPECT_OK;
+}
+
+int spect_backproject(spect_plan_t p, float* image, const float* views, const int32_t* index, int nindex,
+                      void* stream) {
+  if (!p || !views || !image) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int* vi;
+  STATUS_TRY(stage_index(p, index, nindex, st, &vi));
+  return backward(p, image, views, vi, nindex, st, 0, nullptr);
+}
+
+int spect_backproject_host(spect_plan_t p, float* image, const float* views, const int32_t* index, int nindex) {
+  if (!p || !views || !image) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  STATUS_TRY(ensure_io(p));
+  cudaStream_t st = 0;
+  const int* vi;
+  STATUS_TRY(stage_index(p, index, nindex, st, &vi));
+  CUDA_TRY(cudaMemcpyAsync(p->d_io_views, views, sizeof(float) * nindex * p->nxz, cudaMemcpyHostToDevice, st));
+  STATUS_TRY(backward(p, p->d_io_img, p->d_io_views, vi, nindex, st, 0, nullptr));
+  CUDA_TRY(cudaMemcpyAsync(image, p->d_io_img, sizeof(float) * p->N, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SPECT_OK;
+}
+
+int spect_osem(spect_plan_t p, float* out, const float* x0, const float* ynoisy, const float* background, int nblocks,
+               int niter, void* stream) {
+  if (!p || !out || !x0 || !ynoisy || !background) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  return run_osem(p, out, x0, ynoisy, background, nblocks, niter, (cudaStream_t)stream);
+}
+
+int spect_mlem(spect_plan_t p, float* out, const float* x0, const float* ynoisy, const float* background, int niter,
+               void* stream) {
+  return spect_osem(p, out, x0, ynoisy, background, 1, niter, stream);
+}
+
+int spect_osem_host(spect_plan_t p, float* out, const float* x0, const float* ynoisy, const float* background,
+                    int nblocks, int niter) {
+  if (!p || !out || !x0 || !ynoisy || !background) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  size_t V = (size_t)p->nview * p->nxz;
+  for (size_t k = 0; k < V; ++k)
+    if (!(background[k] > 0.f)) return fail(SPECT_ERR_BACKGROUND, "need background > 0");
+  STATUS_TRY(ensure_io(p));
+  cudaStream_t st = 0;
+  float* dx = p->d_io_img;
+  float* dy = p->d_io_views;
+  float* db = p->d_io_views + V;
+  CUDA_TRY(cudaMemcpyAsync(dx, x0, sizeof(float) * p->N, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(dy, ynoisy, sizeof(float) * V, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(db, background, sizeof(float) * V, cudaMemcpyHostToDevice, st));
+  STATUS_TRY(run_osem(p, dx, dx, dy, db, nblocks, niter, st));
+  CUDA_TRY(cudaMemcpyAsync(out, dx, sizeof(float) * p->N, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SPECT_OK;
+}
+
+int spect_mlem_host(spect_plan_t p, float* out, const float* x0, const float* ynoisy, const float* background,
+                    int niter) {
+  return spect_osem_host(p, out, x0, ynoisy, background, 1, niter);
+}
+
+int spect_em_subset_update(spect_plan_t p, float* x, const float* ynoisy, const float* background, const float* asum,
+                           const int32_t* index, int nindex, void* stream) {
+  if (!p || !x || !ynoisy || !background || !asum) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  STATUS_TRY(ensure_em(p, 1));
+  const int* vi;
+  STATUS_TRY(stage_index(p, index, nindex, st, &vi));
+  STATUS_TRY(forward(p, p->d_views_tmp, x, vi, nindex, st, ynoisy, background));
+  return backward(p, x, p->d_views_tmp, vi, nindex, st, 2, asum);
+}
+
+int spect_subset_sensitivity(spect_plan_t p, float* asum, const int32_t* index, int nindex, void* stream) {
+  if (!p || !asum) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  STATUS_TRY(ensure_em(p, 1));
+  const int* vi;
+  STATUS_TRY(stage_index(p, index, nindex, st, &vi));
+  return backward(p, asum, p->d_ones, vi, nindex, st, 1, nullptr);
+}
+
+int spect_psf_gauss(float* psf, int ny, int px, int pz, const double* fwhm_x, const double* fwhm_z) {
+  if (!psf || !fwhm_x || ny <= 0 || px <= 0 || pz <= 0) return fail(SPECT_ERR_ARG, "bad psf_gauss arguments");
+  if (!fwhm_z) fwhm_z = fwhm_x;
+  auto gauss = [](int p, double fwhm, std::vector<double>& w) -> int {
+    w.assign(p, 0.0);
+    int h = (p - 1) / 2;
+    if (fwhm == 0) {  // Kronecker impulse at r == 0
+      bool has0 = false;
+      for (int i = 0; i < p; ++i)
+        if (-h + i == 0) {
+          w[i] = 1.0;
+          has0 = true;
+        }
+      return has0 ? 0 : -1;
+    }
+    double sigma = fwhm / std::sqrt(std::log(256.0));
+    double s = 0;
+    for (int i = 0; i < p; ++i) {
+      double r = (double)(-h + i) / sigma;
+      w[i] = std::exp(-0.5 * r * r);
+      s += w[i];
+    }
+    for (auto& v : w) v /= s;
+    return 0;
+  };
+  std::vector<double> wx, wz;
+  for (int y = 0; y < ny; ++y) {
+    if (gauss(px, fwhm_x[y], wx) || gauss(pz, fwhm_z[y], wz))
+      return fail(SPECT_ERR_ARG, "must have some r=0 if fwhm=0");
+    for (int j = 0; j < pz; ++j)
+      for (int i = 0; i < px; ++i) psf[((size_t)y * pz + j) * px + i] = (float)(wx[i] * wz[j]);
+  }
+  return SPECT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,641 @@
+// spect_kernels.cuh -- sm_100a kernels of the SPECT projector hot path.
+//
+// Forward pass of one group of views (project!, src/project.jl:77-135):
+//   k_rot_fwd    rotate image and mu-map slices about z (imrotate! :two,
+//                src/rotatez.jl:331-362), depth-scan the rotated mu-map and
+//                write P[slot][y][z][x] = exp(-dy*(sum_{j<y} mu_j + mu_y/2)) * R(image)
+//                (src/project.jl:103-116).  One CTA per (z slice, view split);
+//                slices staged in shared memory.
+//   k_conv_fwd   persistent; one work item = (view slot, chunk of depth planes).
+//                Per plane: replicate-padded real z-FFT of row pairs, x-FFT of
+//                every kz column with replicate padding, multiply by the
+//                plane's precomputed real PSF spectrum, inverse x-FFT, crop,
+//                inverse z-FFT, crop, accumulate over depth in shared memory
+//                (fft_conv!, src/fft_convolve.jl:33-55, and the depth sum of
+//                src/project.jl:127-130).
+//   k_reduce_views  sum of the chunk partials in chunk order (+ fused EM ratio).
+// Adjoint pass (backproject!, src/backproject.jl:277-332):
+//   k_vspec      2-D spectrum of each zero-padded view (shared by all planes).
+//   k_conv_adj   persistent; per plane: spectrum * PSF spectrum, inverse x-FFT,
+//                adjoint of replicate padding along x, inverse z-FFT, adjoint
+//                of replicate padding along z (fft_conv_adj!,
+//                src/fft_convolve.jl:82-130) -> T[slot][y][z][x].
+//   k_rot_adj    attenuation weighting and the exact transpose of the
+//                bilinear rotation (imrotate_adj! :two, src/rotatez.jl:390-416),
+//                atomic-free: rotated-grid points are scattered in 9 passes by
+//                lattice class (o1 mod 3, o2 mod 3), inside which footprints
+//                are disjoint.  Per-view sums in view order.
+//   k_reduce_image  sum of split partials (+ fused EM multiplicative update).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_warp.cuh"
+
+namespace spect {
+
+constexpr int kConvThreads = 512;
+constexpr int kConvWarps = kConvThreads / 32;
+
+struct Geom {
+  int nx, ny, nz;
+  int Npx, Npz, logNpx, logNpz, Hz;  // padded FFT sizes (src/helper.jl:8-12), Hz = Npz/2+1
+  int padup, padleft;                // _padup(nx,px), _padleft(nz,pz)
+  float dy;
+  float c0;                          // rotation centre (nx-1)/2, 0-based unpadded
+};
+
+// Per-view rotation: x = cos(2pi - theta), y = sin(2pi - theta) rounded to
+// float; z = 1 when theta == 0 mod 2pi (the forward :two shortcut copies).
+struct RotPos {
+  float cs, sn, c0;
+  __device__ __forceinline__ void pos(int i, int j, float& s1, float& s2) const {
+    float di = __fsub_rn((float)i, c0), dj = __fsub_rn((float)j, c0);
+    float a = __fmul_rn(cs, di), b = __fmul_rn(sn, dj), c = __fmul_rn(sn, di), d = __fmul_rn(cs, dj);
+    s1 = __fadd_rn(c0, __fsub_rn(a, b));
+    s2 = __fadd_rn(c0, __fadd_rn(c, d));
+  }
+};
+
+// bilinear sample of a zero-extended n x n slice at output pixel (i, j)
+__device__ __forceinline__ float bilinear(const float* __restrict__ s, int n, const RotPos& R, int i, int j) {
+  float s1, s2;
+  R.pos(i, j, s1, s2);
+  float f1 = floorf(s1), f2 = floorf(s2);
+  int j1 = (int)f1, j2 = (int)f2;
+  float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
+  float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
+  bool x0 = (unsigned)j1 < (unsigned)n, x1 = (unsigned)(j1 + 1) < (unsigned)n;
+  bool y0 = (unsigned)j2 < (unsigned)n, y1 = (unsigned)(j2 + 1) < (unsigned)n;
+  float a = (x0 && y0) ? s[j1 + j2 * n] : 0.f;
+  float b = (x1 && y0) ? s[j1 + 1 + j2 * n] : 0.f;
+  float c = (x0 && y1) ? s[j1 + (j2 + 1) * n] : 0.f;
+  float d = (x1 && y1) ? s[j1 + 1 + (j2 + 1) * n] : 0.f;
+  float v = __fmul_rn(__fmul_rn(u1, u2), a);
+  v = __fadd_rn(v, __fmul_rn(__fmul_rn(t1, u2), b));
+  v = __fadd_rn(v, __fmul_rn(__fmul_rn(u1, t2), c));
+  v = __fadd_rn(v, __fmul_rn(__fmul_rn(t1, t2), d));
+  return v;
+}
+
+// ------------------------------------------------------------------------
+// k_rot_fwd: grid (nz, nsplit), block nx * vpb threads.
+// P[slot][y][z][x] for slots [split range).  SMEM: stage the two slices.
+template <bool SMEM>
+__global__ void __launch_bounds__(1024) k_rot_fwd(Geom g, const float* __restrict__ image,
+                                                  const float* __restrict__ mumap, const float4* __restrict__ rot,
+                                                  const int* __restrict__ vidx, int nv, float* __restrict__ P) {
+  extern __shared__ float4 smem4[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int z = blockIdx.x;
+  const size_t slice = (size_t)nx * ny;
+  const float* img = image + (size_t)z * slice;
+  const float* mu = mumap + (size_t)z * slice;
+  if (SMEM) {
+    float* si = reinterpret_cast<float*>(smem4);
+    float* sm = si + slice;
+    for (int k = threadIdx.x; k < (int)slice; k += blockDim.x) {
+      si[k] = __ldg(img + k);
+      sm[k] = __ldg(mu + k);
+    }
+    __syncthreads();
+    img = si;
+    mu = sm;
+  }
+  const int per = (nv + gridDim.y - 1) / gridDim.y;
+  const int s0 = blockIdx.y * per, s1 = min(nv, s0 + per);
+  const int vpb = blockDim.x / nx;
+  const int sub = threadIdx.x / nx, x = threadIdx.x - sub * nx;
+  if (sub >= vpb) return;
+  const float mdy = -g.dy;
+  for (int s = s0 + sub; s < s1; s += vpb) {
+    const float4 r = rot[vidx[s]];
+    RotPos R{r.x, r.y, g.c0};
+    const bool ident = r.z != 0.f;
+    float prefix = 0.f;
+    float* out = P + ((size_t)s * ny * nz + z) * nx + x;
+    for (int y = 0; y < ny; ++y) {
+      float f, m;
+      if (ident) {
+        f = img[x + y * nx];
+        m = mu[x + y * nx];
+      } else {
+        f = bilinear(img, nx, R, x, y);
+        m = bilinear(mu, nx, R, x, y);
+      }
+      // exp(-dy * (sum_{j<y} mu_j + mu_y/2))  (src/project.jl:103-113)
+      float e = __fadd_rn(prefix, __fmul_rn(0.5f, m));
+      float a = expf(__fmul_rn(e, mdy));
+      out[(size_t)y * nz * nx] = __fmul_rn(f, a);
+      prefix = __fadd_rn(prefix, m);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+struct ConvArgs {
+  Geom g;
+  const float* P;       // forward: [nv][ny][nz][nx] rotated+attenuated planes
+  float* T;             // adjoint: [nv][ny][nz][nx] output planes
+  const float* H;       // [nset][ny][Hz][Npx] real PSF spectra (scaled by 1/(Npx*Npz))
+  const int* vidx;      // [nv] plan view index of each slot
+  const int* viewset;   // [nview] spectrum set of each plan view
+  const float2* Vhat;   // adjoint: [nv][Hz][Npx] view spectra
+  float2* VhatOut;      // k_vspec output
+  const float* views;   // k_vspec input [nv][nz][nx]
+  int nv, chunkY, nchunks;
+  float* part;          // forward: [nv][nchunks][nz][nx]
+  float2* gB;           // global fallback for B, per CTA nx*Hz
+  float* gacc;          // global fallback for acc/tbuf, per CTA nz*(nx+2)
+  const float2* tw;     // twiddle table (global)
+  int bsmem, asmem;     // whether B / acc live in shared memory
+};
+
+struct ConvSmem {
+  float2* tw;
+  float2* scratch;  // this warp's line buffer
+  float2* B;        // nx rows x Hz complex (mixed domain: x spatial, kz frequency)
+  float* acc;       // nz x (nx+2) accumulator / output staging
+};
+
+__device__ __forceinline__ ConvSmem conv_smem_setup(const ConvArgs& a, int maxN) {
+  extern __shared__ float4 smem4[];
+  ConvSmem s;
+  const int warp = threadIdx.x >> 5;
+  s.tw = reinterpret_cast<float2*>(smem4);
+  float2* scr = s.tw + SPECT_TW_N;
+  s.scratch = scr + warp * maxN;
+  float2* after = scr + kConvWarps * maxN;
+  size_t Bn = (size_t)a.g.nx * a.g.Hz;
+  if (a.bsmem) {
+    s.B = after;
+    after += Bn;
+  } else {
+    s.B = a.gB + (size_t)blockIdx.x * Bn;
+  }
+  size_t An = (size_t)a.g.nz * (a.g.nx + 2);
+  if (a.asmem) s.acc = reinterpret_cast<float*>(after);
+  else s.acc = a.gacc + (size_t)blockIdx.x * An;
+  for (int k = threadIdx.x; k < SPECT_TW_N; k += blockDim.x) s.tw[k] = a.tw[k];
+  __syncthreads();
+  return s;
+}
+
+// z-FFT of row pairs (x0, x0+1) read from real rows of B (row stride 2*Hz
+// floats); ZEROPAD selects zero padding (adjoint) instead of replication.
+template <bool ZEROPAD>
+__device__ __forceinline__ void stage_zfft_rows(const Geom& g, ConvSmem& s, int warp, int lane) {
+  const int Hz = g.Hz, Npz = g.Npz, nz = g.nz, nx = g.nx;
+  float* Bf = reinterpret_cast<float*>(s.B);
+  for (int rp = warp; rp < (nx >> 1); rp += kConvWarps) {
+    const int x0 = 2 * rp;
+    const float* r0 = Bf + (size_t)x0 * 2 * Hz;
+    const float* r1 = r0 + 2 * Hz;
+    for (int zz = lane; zz < Npz; zz += 32) {
+      int zc = zz - g.padleft;
+      float2 v;
+      if (ZEROPAD) {
+        bool in = (unsigned)zc < (unsigned)nz;
+        v = in ? make_float2(r0[zc], r1[zc]) : make_float2(0.f, 0.f);
+      } else {
+        zc = min(max(zc, 0), nz - 1);
+        v = make_float2(r0[zc], r1[zc]);
+      }
+      s.scratch[zz] = v;
+    }
+    __syncwarp();
+    warp_fft<false>(s.scratch, Npz, g.logNpz, s.tw, lane);
+    // unpack the two real rows: A[k] = (Z[k] + conj Z[-k]) / 2, B[k] = (Z[k] - conj Z[-k]) / 2i
+    for (int k = lane; k < Hz; k += 32) {
+      float2 zk = s.scratch[k], zn = s.scratch[(Npz - k) & (Npz - 1)];
+      s.B[(size_t)x0 * Hz + k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+      s.B[(size_t)(x0 + 1) * Hz + k] = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
+    }
+    __syncwarp();
+  }
+}
+
+// transposed load of a real nz x nx plane (x fastest in memory) into the real
+// rows of B: Bf[x][z].
+__device__ __forceinline__ void stage_load_plane(const Geom& g, ConvSmem& s, const float* __restrict__ src) {
+  float* Bf = reinterpret_cast<float*>(s.B);
+  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.Hz;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    int z = k / nx, x = k - z * nx;
+    Bf[(size_t)x * rs + z] = __ldg(src + k);
+  }
+}
+
+// build the Hermitian-extended spectrum of the row pair (x0, x0+1) in scratch
+__device__ __forceinline__ void hermitian_pair(const Geom& g, ConvSmem& s, int x0, int lane) {
+  const int Hz = g.Hz, Npz = g.Npz;
+  const float2* b0 = s.B + (size_t)x0 * Hz;
+  const float2* b1 = b0 + Hz;
+  for (int k = lane; k < Npz; k += 32) {
+    float2 a, b;
+    if (k < Hz) {
+      a = b0[k];
+      b = b1[k];
+      if (k == 0 || k == Hz - 1) {  // DC / Nyquist bins of a real row are real
+        a.y = 0.f;
+        b.y = 0.f;
+      }
+    } else {
+      a = b0[Npz - k];
+      b = b1[Npz - k];
+      a.y = -a.y;
+      b.y = -b.y;
+    }
+    s.scratch[k] = make_float2(a.x - b.y, a.y + b.x);  // a + i b
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ------------------------------------------------------------------------
+// k_conv_fwd: persistent over items (slot, chunk).
+__global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd(ConvArgs a) {
+  const Geom& g = a.g;
+  const int maxN = max(g.Npx, g.Npz);
+  ConvSmem s = conv_smem_setup(a, maxN);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, Hz = g.Hz, Npx = g.Npx;
+  const int AS = nx + 2;
+  const int nitems = a.nv * a.nchunks;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int slot = item / a.nchunks, c = item - slot * a.nchunks;
+    const int y0 = c * a.chunkY, y1 = min(ny, y0 + a.chunkY);
+    const float* Pv = a.P + (size_t)slot * ny * nz * nx;
+    const float* Hv = a.H + (size_t)a.viewset[a.vidx[slot]] * ny * Hz * Npx;
+    for (int y = y0; y < y1; ++y) {
+      __syncthreads();  // B and scratch free
+      stage_load_plane(g, s, Pv + (size_t)y * nz * nx);
+      __syncthreads();
+      stage_zfft_rows<false>(g, s, warp, lane);
+      __syncthreads();
+      // x-FFT per kz column, multiply by the PSF spectrum, inverse, crop
+      const float* Hy = Hv + (size_t)y * Hz * Npx;
+      for (int kz = warp; kz < Hz; kz += kConvWarps) {
+        for (int xx = lane; xx < Npx; xx += 32) {
+          int xc = min(max(xx - g.padup, 0), nx - 1);
+          s.scratch[xx] = s.B[(size_t)xc * Hz + kz];
+        }
+        __syncwarp();
+        warp_fft<false>(s.scratch, Npx, g.logNpx, s.tw, lane);
+        const float* h = Hy + (size_t)kz * Npx;
+        for (int kx = lane; kx < Npx; kx += 32) {
+          float hv = __ldg(h + kx);
+          float2 v = s.scratch[kx];
+          s.scratch[kx] = make_float2(v.x * hv, v.y * hv);
+        }
+        __syncwarp();
+        warp_fft<true>(s.scratch, Npx, g.logNpx, s.tw, lane);
+        for (int x = lane; x < nx; x += 32) s.B[(size_t)x * Hz + kz] = s.scratch[g.padup + x];
+        __syncwarp();
+      }
+      __syncthreads();
+      // inverse z-FFT of row pairs, crop, accumulate over depth
+      const bool first = (y == y0);
+      for (int rp = warp; rp < (nx >> 1); rp += kConvWarps) {
+        const int x0 = 2 * rp;
+        hermitian_pair(g, s, x0, lane);
+        warp_fft<true>(s.scratch, g.Npz, g.logNpz, s.tw, lane);
+        for (int z = lane; z < nz; z += 32) {
+          float2 r = s.scratch[g.padleft + z];
+          float2* o = reinterpret_cast<float2*>(s.acc + (size_t)z * AS + x0);
+          if (first) {
+            *o = r;
+          } else {
+            float2 p = *o;
+            *o = make_float2(p.x + r.x, p.y + r.y);
+          }
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    float* dst = a.part + ((size_t)slot * a.nchunks + c) * nz * nx;
+    for (int k = threadIdx.x; k < nz * nx; k += blockDim.x) {
+      int z = k / nx, x = k - z * nx;
+      dst[k] = s.acc[(size_t)z * AS + x];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// k_vspec: spectrum of each zero-padded view, Vhat[slot][kz][kx].
+__global__ void __launch_bounds__(kConvThreads, 1) k_vspec(ConvArgs a) {
+  const Geom& g = a.g;
+  const int maxN = max(g.Npx, g.Npz);
+  ConvSmem s = conv_smem_setup(a, maxN);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = g.nx, nz = g.nz, Hz = g.Hz, Npx = g.Npx;
+  for (int slot = blockIdx.x; slot < a.nv; slot += gridDim.x) {
+    __syncthreads();
+    stage_load_plane(g, s, a.views + (size_t)slot * nz * nx);
+    __syncthreads();
+    stage_zfft_rows<true>(g, s, warp, lane);
+    __syncthreads();
+    for (int kz = warp; kz < Hz; kz += kConvWarps) {
+      for (int xx = lane; xx < Npx; xx += 32) {
+        int xc = xx - g.padup;
+        s.scratch[xx] = ((unsigned)xc < (unsigned)nx) ? s.B[(size_t)xc * Hz + kz] : make_float2(0.f, 0.f);
+      }
+      __syncwarp();
+      warp_fft<false>(s.scratch, Npx, g.logNpx, s.tw, lane);
+      float2* out = a.VhatOut + ((size_t)slot * Hz + kz) * Npx;
+      for (int kx = lane; kx < Npx; kx += 32) out[kx] = s.scratch[kx];
+      __syncwarp();
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// k_conv_adj: persistent over items (slot, chunk); T[slot][y][z][x].
+__global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj(ConvArgs a) {
+  const Geom& g = a.g;
+  const int maxN = max(g.Npx, g.Npz);
+  ConvSmem s = conv_smem_setup(a, maxN);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, Hz = g.Hz, Npx = g.Npx, Npz = g.Npz;
+  const int AS = nx + 2;
+  const int nitems = a.nv * a.nchunks;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int slot = item / a.nchunks, c = item - slot * a.nchunks;
+    const int y0 = c * a.chunkY, y1 = min(ny, y0 + a.chunkY);
+    const float* Hv = a.H + (size_t)a.viewset[a.vidx[slot]] * ny * Hz * Npx;
+    const float2* Vs = a.Vhat + (size_t)slot * Hz * Npx;
+    for (int y = y0; y < y1; ++y) {
+      __syncthreads();
+      const float* Hy = Hv + (size_t)y * Hz * Npx;
+      for (int kz = warp; kz < Hz; kz += kConvWarps) {
+        const float* h = Hy + (size_t)kz * Npx;
+        const float2* vk = Vs + (size_t)kz * Npx;
+        for (int kx = lane; kx < Npx; kx += 32) {
+          float hv = __ldg(h + kx);
+          float2 v = vk[kx];
+          s.scratch[kx] = make_float2(v.x * hv, v.y * hv);
+        }
+        __syncwarp();
+        warp_fft<true>(s.scratch, Npx, g.logNpx, s.tw, lane);
+        // adjoint of replicate padding along x: fold the pad rows into the edges
+        float lr = 0.f, li = 0.f, hr = 0.f, hi = 0.f;
+        for (int xx = lane; xx < g.padup; xx += 32) {
+          float2 v = s.scratch[xx];
+          lr += v.x;
+          li += v.y;
+        }
+        for (int xx = g.padup + nx + lane; xx < Npx; xx += 32) {
+          float2 v = s.scratch[xx];
+          hr += v.x;
+          hi += v.y;
+        }
+        lr = warp_sum(lr);
+        li = warp_sum(li);
+        hr = warp_sum(hr);
+        hi = warp_sum(hi);
+        for (int x = lane; x < nx; x += 32) {
+          float2 v = s.scratch[g.padup + x];
+          if (x == 0) {
+            v.x += lr;
+            v.y += li;
+          }
+          if (x == nx - 1) {
+            v.x += hr;
+            v.y += hi;
+          }
+          s.B[(size_t)x * Hz + kz] = v;
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+      for (int rp = warp; rp < (nx >> 1); rp += kConvWarps) {
+        const int x0 = 2 * rp;
+        hermitian_pair(g, s, x0, lane);
+        warp_fft<true>(s.scratch, Npz, g.logNpz, s.tw, lane);
+        float lr = 0.f, li = 0.f, hr = 0.f, hi = 0.f;
+        for (int zz = lane; zz < g.padleft; zz += 32) {
+          float2 v = s.scratch[zz];
+          lr += v.x;
+          li += v.y;
+        }
+        for (int zz = g.padleft + nz + lane; zz < Npz; zz += 32) {
+          float2 v = s.scratch[zz];
+          hr += v.x;
+          hi += v.y;
+        }
+        lr = warp_sum(lr);
+        li = warp_sum(li);
+        hr = warp_sum(hr);
+        hi = warp_sum(hi);
+        for (int z = lane; z < nz; z += 32) {
+          float2 v = s.scratch[g.padleft + z];
+          if (z == 0) {
+            v.x += lr;
+            v.y += li;
+          }
+          if (z == nz - 1) {
+            v.x += hr;
+            v.y += hi;
+          }
+          *reinterpret_cast<float2*>(s.acc + (size_t)z * AS + x0) = v;
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+      float* dst = a.T + ((size_t)slot * ny + y) * nz * nx;
+      for (int k = threadIdx.x; k < nz * nx; k += blockDim.x) {
+        int z = k / nx, x = k - z * nx;
+        dst[k] = s.acc[(size_t)z * AS + x];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// k_reduce_views: out[slot] = sum_c part[slot][c]; with EM, out = y/(sum+bg)
+__global__ void k_reduce_views(const float* __restrict__ part, int nv, int nchunks, int nxz,
+                               float* __restrict__ out, const float* __restrict__ y, const float* __restrict__ bg,
+                               const int* __restrict__ vidx) {
+  const size_t n = (size_t)nv * nxz;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    size_t slot = k / nxz, e = k - slot * nxz;
+    const float* p = part + slot * nchunks * nxz + e;
+    float sacc = p[0];
+    for (int c = 1; c < nchunks; ++c) sacc += p[(size_t)c * nxz];
+    if (y) {
+      size_t src = (size_t)vidx[slot] * nxz + e;
+      sacc = y[src] / (sacc + bg[src]);
+    }
+    out[k] = sacc;
+  }
+}
+
+// ------------------------------------------------------------------------
+// k_rot_adj: grid (nz, nsplit), block kRotAdjThreads.  Accumulates
+// sum_s R'(a_s .* T_s) for the slots of this split into acc (shared or the
+// global per-CTA buffer) and adds/writes it into imgpart[split][z][:][:].
+constexpr int kRotAdjThreads = 512;
+
+__global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const float* __restrict__ T,
+                                                                const float* __restrict__ mumap,
+                                                                const float4* __restrict__ rot,
+                                                                const int* __restrict__ vidx, int nv,
+                                                                float* __restrict__ imgpart, int accumulate,
+                                                                int use_smem, float* __restrict__ gscr) {
+  extern __shared__ float4 smem4[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int z = blockIdx.x, split = blockIdx.y;
+  const int slice = nx * ny;
+  float* acc;
+  float* S;
+  float* segsum;
+  const int nseg = max(1, (int)blockDim.x / nx);
+  if (use_smem) {
+    acc = reinterpret_cast<float*>(smem4);
+    S = acc + slice;
+    segsum = S + slice;
+  } else {
+    size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+    acc = gscr + cta * (2 * (size_t)slice + (size_t)nseg * nx);
+    S = acc + slice;
+    segsum = S + slice;
+  }
+  float* outp = imgpart + ((size_t)split * nz + z) * slice;
+  for (int k = threadIdx.x; k < slice; k += blockDim.x) acc[k] = accumulate ? outp[k] : 0.f;
+  const float* mu = mumap + (size_t)z * slice;
+  const int per = (nv + gridDim.y - 1) / gridDim.y;
+  const int s0 = split * per, s1 = min(nv, s0 + per);
+  const float mdy = -g.dy;
+  const int seglen = (ny + nseg - 1) / nseg;
+  const int myseg = threadIdx.x / nx, o1s = threadIdx.x - myseg * nx;
+  for (int s = s0; s < s1; ++s) {
+    const float4 r = rot[vidx[s]];
+    RotPos R{r.x, r.y, g.c0};
+    const bool ident = r.z != 0.f;
+    __syncthreads();
+    // 1) rotated mu-map of this view on the rotated grid (forward sampling)
+    for (int k = threadIdx.x; k < slice; k += blockDim.x) {
+      int o2 = k / nx, o1 = k - o2 * nx;
+      S[k] = ident ? __ldg(mu + k) : bilinear(mu, nx, R, o1, o2);
+    }
+    __syncthreads();
+    // 2) depth scan along o2 (= y) per column o1, attenuation, times T
+    if (myseg < nseg) {
+      const int ya = myseg * seglen, yb = min(ny, ya + seglen);
+      float sum = 0.f;
+      for (int y = ya; y < yb; ++y) sum = __fadd_rn(sum, S[y * nx + o1s]);
+      segsum[myseg * nx + o1s] = sum;
+    }
+    __syncthreads();
+    if (myseg < nseg) {
+      const int ya = myseg * seglen, yb = min(ny, ya + seglen);
+      float prefix = 0.f;
+      for (int q = 0; q < myseg; ++q) prefix = __fadd_rn(prefix, segsum[q * nx + o1s]);
+      const float* Tc = T + ((size_t)s * ny * nz + z) * nx + o1s;
+      for (int y = ya; y < yb; ++y) {
+        float m = S[y * nx + o1s];
+        float e = __fadd_rn(prefix, __fmul_rn(0.5f, m));
+        float at = expf(__fmul_rn(e, mdy));
+        S[y * nx + o1s] = __fmul_rn(at, __ldg(Tc + (size_t)y * nz * nx));
+        prefix = __fadd_rn(prefix, m);
+      }
+    }
+    __syncthreads();
+    // 3) transpose of the bilinear sampling, 9 disjoint lattice classes
+    for (int cls = 0; cls < 9; ++cls) {
+      const int c1 = cls % 3, c2 = cls / 3;
+      const int n1 = (nx - c1 + 2) / 3, n2 = (ny - c2 + 2) / 3;
+      for (int k = threadIdx.x; k < n1 * n2; k += blockDim.x) {
+        int q2 = k / n1, q1 = k - q2 * n1;
+        int o1 = c1 + 3 * q1, o2 = c2 + 3 * q2;
+        float val = S[o1 + o2 * nx];
+        float s1, s2;
+        R.pos(o1, o2, s1, s2);
+        float f1 = floorf(s1), f2 = floorf(s2);
+        int j1 = (int)f1, j2 = (int)f2;
+        float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
+        float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
+        bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
+        bool y0 = (unsigned)j2 < (unsigned)ny, y1 = (unsigned)(j2 + 1) < (unsigned)ny;
+        if (x0 && y0) acc[j1 + j2 * nx] += __fmul_rn(__fmul_rn(u1, u2), val);
+        if (x1 && y0) acc[j1 + 1 + j2 * nx] += __fmul_rn(__fmul_rn(t1, u2), val);
+        if (x0 && y1) acc[j1 + (j2 + 1) * nx] += __fmul_rn(__fmul_rn(u1, t2), val);
+        if (x1 && y1) acc[j1 + 1 + (j2 + 1) * nx] += __fmul_rn(__fmul_rn(t1, t2), val);
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < slice; k += blockDim.x) outp[k] = acc[k];
+}
+
+// k_reduce_image: img = sum_split imgpart[split]; EM: x .*= img ./ asum
+__global__ void k_reduce_image(const float* __restrict__ imgpart, int nsplit, size_t N, float* __restrict__ out,
+                               const float* __restrict__ asum, int em_update, int inf_zero) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < N; k += (size_t)gridDim.x * blockDim.x) {
+    float v = imgpart[k];
+    for (int s = 1; s < nsplit; ++s) v += imgpart[(size_t)s * N + k];
+    if (inf_zero && v == 0.f) v = __int_as_float(0x7f800000);  // asum zeros -> Inf
+    if (em_update) out[k] = out[k] * (v / asum[k]);
+    else out[k] = v;
+  }
+}
+
+// ------------------------------------------------------------------------
+// PSF spectra: H[set][y][kz][kx] = Re sum_{d,e} h[d,e] w_x^{kx d} w_z^{kz e} / (Npx Npz)
+// with h[d,e] = psf[(pz-1)/2+e][(px-1)/2+d], the circularly centred kernel
+// (pad2sizezero! + fftshift2!, src/helper.jl:66-80, 111-142).  Double math.
+__global__ void k_psf_stage1(const float* __restrict__ psf, int nplanes, int px, int pz, int Npx,
+                             const double2* __restrict__ wx, double2* __restrict__ G) {
+  // G[pl][e][kx] = sum_d h[d,e] w_x^{(kx*d) mod Npx}
+  const size_t n = (size_t)nplanes * pz * Npx;
+  const int cx = (px - 1) / 2;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int kx = (int)(k % Npx);
+    size_t r = k / Npx;
+    int e = (int)(r % pz);
+    size_t pl = r / pz;
+    const float* row = psf + (pl * pz + e) * px;
+    double re = 0, im = 0;
+    for (int a = 0; a < px; ++a) {
+      int d = a - cx;
+      int m = (int)(((long long)kx * d) % Npx);
+      if (m < 0) m += Npx;
+      double2 w = wx[m];
+      double h = (double)row[a];
+      re += h * w.x;
+      im += h * w.y;
+    }
+    G[k] = make_double2(re, im);
+  }
+}
+
+__global__ void k_psf_stage2(const double2* __restrict__ G, int nplanes, int pz, int Npx, int Npz, int Hz,
+                             const double2* __restrict__ wz, float* __restrict__ H) {
+  const size_t n = (size_t)nplanes * Hz * Npx;
+  const int cz = (pz - 1) / 2;
+  const double scale = 1.0 / ((double)Npx * Npz);
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int kx = (int)(k % Npx);
+    size_t r = k / Npx;
+    int kz = (int)(r % Hz);
+    size_t pl = r / Hz;
+    double re = 0;
+    for (int b = 0; b < pz; ++b) {
+      int e = b - cz;
+      int m = (int)(((long long)kz * e) % Npz);
+      if (m < 0) m += Npz;
+      double2 w = wz[m], gv = G[(pl * pz + b) * Npx + kx];
+      re += gv.x * w.x - gv.y * w.y;
+    }
+    H[k] = (float)(re * scale);
+  }
+}
+
+}  // namespace spect
