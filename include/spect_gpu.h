@@ -132,6 +132,18 @@ int spect_em_subset_update(spect_plan_t plan, float* x, const float* ynoisy, con
 int spect_subset_sensitivity(spect_plan_t plan, float* asum, const int32_t* index, int nindex,
                              void* stream);
 
+/* Kernel accounting (no counterpart in the reference; measurement support).
+ * spect_kernel_launches: number of kernels this library has launched in the
+ * process.  spect_plan_profile(plan, on): when on, every kernel the plan
+ * launches is bracketed by CUDA events on its stream; spect_plan_kernel_times
+ * synchronises on those events and returns, per kernel kind, the summed
+ * device milliseconds and launch counts since profiling was switched on:
+ * index 0 k_rot_fwd, 1 k_conv_fwd, 2 k_reduce_views, 3 k_vspec,
+ * 4 k_conv_adj, 5 k_rot_adj, 6 k_reduce_image, 7 other. */
+unsigned long long spect_kernel_launches(void);
+int spect_plan_profile(spect_plan_t plan, int on);
+int spect_plan_kernel_times(spect_plan_t plan, double ms[8], long long counts[8]);
+
 /* psf_gauss(; ny, px, pz, fwhm_x, fwhm_z) (src/psf-gauss.jl:24-55): host
  * generator of depth-dependent Gaussian PSFs into psf[ny][pz][px] (Julia
  * psf[px,pz,ny]).  fwhm_x/fwhm_z hold ny values (fwhm_z NULL = fwhm_x). */

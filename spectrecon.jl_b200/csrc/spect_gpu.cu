@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -70,6 +71,60 @@ inline int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 constexpr double kTwoPi = 6.283185307179586;
 
+std::atomic<unsigned long long> g_launches{0};
+
+enum KernelKind { K_ROT_FWD, K_CONV_FWD, K_REDUCE_VIEWS, K_VSPEC, K_CONV_ADJ, K_ROT_ADJ, K_REDUCE_IMAGE, K_OTHER,
+                  K_KINDS };
+
+// CUDA-event bracketing of every launch of a plan (measurement support)
+struct Profiler {
+  bool on = false;
+  struct Rec {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> pending;
+  std::vector<cudaEvent_t> pool;
+  double ms[K_KINDS] = {0};
+  long long n[K_KINDS] = {0};
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void drain() {
+    for (auto& r : pending) {
+      cudaEventSynchronize(r.b);
+      float t = 0;
+      cudaEventElapsedTime(&t, r.a, r.b);
+      ms[r.kind] += t;
+      n[r.kind] += 1;
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    pending.clear();
+  }
+  void reset() {
+    drain();
+    for (int k = 0; k < K_KINDS; ++k) {
+      ms[k] = 0;
+      n[k] = 0;
+    }
+  }
+  ~Profiler() {
+    for (auto& r : pending) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
 }  // namespace
 
 struct spect_plan_s {
@@ -116,6 +171,7 @@ struct spect_plan_s {
   int rota_smem_ok = 1, nsplit_adj = 1;
   size_t rota_smem = 0;
   size_t bytes = 0;
+  Profiler prof;
   std::mutex mu;
 };
 
@@ -146,10 +202,28 @@ void free_plan(spect_plan_s* p) {
 }
 
 int check_launch(const char* what) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
   return SPECT_OK;
 }
+
+// LAUNCH(plan, kind, stream, name, <kernel launch expression>)
+#define LAUNCH(P, KIND, ST, NAME, ...)                   \
+  do {                                                   \
+    cudaEvent_t ea_ = nullptr, eb_ = nullptr;            \
+    if ((P)->prof.on) {                                  \
+      ea_ = (P)->prof.get();                             \
+      eb_ = (P)->prof.get();                             \
+      cudaEventRecord(ea_, ST);                          \
+    }                                                    \
+    __VA_ARGS__;                                         \
+    if ((P)->prof.on) {                                  \
+      cudaEventRecord(eb_, ST);                          \
+      (P)->prof.pending.push_back({KIND, ea_, eb_});     \
+    }                                                    \
+    STATUS_TRY(check_launch(NAME));                      \
+  } while (0)
 
 // Launch configuration that depends only on the plan's sizes.
 int configure(spect_plan_s* p) {
@@ -249,11 +323,10 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
     int vpb = p->rotf_vpb;
     int nsplit = std::max(1, std::min(cdiv(2 * p->sm_count, g.nz), cdiv(nv, vpb)));
     dim3 grid(g.nz, nsplit);
-    if (p->rotf_smem_ok)
-      k_rot_fwd<true><<<grid, g.nx * vpb, p->rotf_smem, st>>>(g, image, p->d_mumap, p->d_rot, vi, nv, p->d_P);
-    else
-      k_rot_fwd<false><<<grid, g.nx * vpb, 0, st>>>(g, image, p->d_mumap, p->d_rot, vi, nv, p->d_P);
-    STATUS_TRY(check_launch("k_rot_fwd"));
+    LAUNCH(p, K_ROT_FWD, st, "k_rot_fwd",
+           if (p->rotf_smem_ok) k_rot_fwd<true><<<grid, g.nx * vpb, p->rotf_smem, st>>>(g, image, p->d_mumap,
+                                                                                         p->d_rot, vi, nv, p->d_P);
+           else k_rot_fwd<false><<<grid, g.nx * vpb, 0, st>>>(g, image, p->d_mumap, p->d_rot, vi, nv, p->d_P));
     // FFT convolution + depth sum -> part
     ConvArgs a = conv_args(p);
     int cy, nc;
@@ -265,13 +338,13 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
     a.nchunks = nc;
     a.part = p->d_part;
     int gridc = std::min(p->conv_grid, nv * nc);
-    k_conv_fwd<<<gridc, kConvThreads, p->conv_smem, st>>>(a);
-    STATUS_TRY(check_launch("k_conv_fwd"));
+    LAUNCH(p, K_CONV_FWD, st, "k_conv_fwd", k_conv_fwd<<<gridc, kConvThreads, p->conv_smem, st>>>(a));
     // chunk sum (+ EM ratio) -> views
     size_t n = (size_t)nv * p->nxz;
     int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16);
-    k_reduce_views<<<rb, 256, 0, st>>>(p->d_part, nv, nc, (int)p->nxz, views + (size_t)g0 * p->nxz, y, bg, vi);
-    STATUS_TRY(check_launch("k_reduce_views"));
+    LAUNCH(p, K_REDUCE_VIEWS, st, "k_reduce_views",
+           k_reduce_views<<<rb, 256, 0, st>>>(p->d_part, nv, nc, (int)p->nxz, views + (size_t)g0 * p->nxz, y, bg,
+                                              vi));
   }
   return SPECT_OK;
 }
@@ -294,24 +367,25 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     a.VhatOut = p->d_Vhat;
     a.nv = nv;
     a.vidx = vi;
-    k_vspec<<<std::min(p->conv_grid, nv), kConvThreads, p->conv_smem, st>>>(a);
-    STATUS_TRY(check_launch("k_vspec"));
+    LAUNCH(p, K_VSPEC, st, "k_vspec", k_vspec<<<std::min(p->conv_grid, nv), kConvThreads, p->conv_smem, st>>>(a));
     int cy, nc;
     chunking(p, nv, &cy, &nc);
     a.Vhat = p->d_Vhat;
     a.T = p->d_P;
     a.chunkY = cy;
     a.nchunks = nc;
-    k_conv_adj<<<std::min(p->conv_grid, nv * nc), kConvThreads, p->conv_smem, st>>>(a);
-    STATUS_TRY(check_launch("k_conv_adj"));
+    LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj",
+           k_conv_adj<<<std::min(p->conv_grid, nv * nc), kConvThreads, p->conv_smem, st>>>(a));
     dim3 grid(g.nz, nsplit);
-    k_rot_adj<<<grid, kRotAdjThreads, p->rota_smem_ok ? p->rota_smem : 0, st>>>(
-        g, p->d_P, p->d_mumap, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok, p->d_gscr_adj);
-    STATUS_TRY(check_launch("k_rot_adj"));
+    LAUNCH(p, K_ROT_ADJ, st, "k_rot_adj",
+           k_rot_adj<<<grid, kRotAdjThreads, p->rota_smem_ok ? p->rota_smem : 0, st>>>(
+               g, p->d_P, p->d_mumap, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
+               p->d_gscr_adj));
   }
   int rb = (int)std::min<size_t>((p->N + 255) / 256, (size_t)p->sm_count * 16);
-  k_reduce_image<<<rb, 256, 0, st>>>(p->d_imgpart, nsplit, p->N, image, asum, mode == 2 ? 1 : 0, mode == 1 ? 1 : 0);
-  STATUS_TRY(check_launch("k_reduce_image"));
+  LAUNCH(p, K_REDUCE_IMAGE, st, "k_reduce_image",
+         k_reduce_image<<<rb, 256, 0, st>>>(p->d_imgpart, nsplit, p->N, image, asum, mode == 2 ? 1 : 0,
+                                            mode == 1 ? 1 : 0));
   return SPECT_OK;
 }
 
@@ -361,8 +435,8 @@ __global__ void k_all_positive(const float* __restrict__ b, size_t n, int* flag)
 int check_background(spect_plan_s* p, const float* bg, cudaStream_t st) {
   size_t V = (size_t)p->nview * p->nxz;
   CUDA_TRY(cudaMemsetAsync(p->d_flag, 0, sizeof(int), st));
-  k_all_positive<<<std::max(1, std::min(cdiv(V, 256), p->sm_count * 8)), 256, 0, st>>>(bg, V, p->d_flag);
-  STATUS_TRY(check_launch("k_all_positive"));
+  LAUNCH(p, K_OTHER, st, "k_all_positive",
+         k_all_positive<<<std::max(1, std::min(cdiv(V, 256), p->sm_count * 8)), 256, 0, st>>>(bg, V, p->d_flag));
   int h = 0;
   CUDA_TRY(cudaMemcpyAsync(&h, p->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -710,6 +784,27 @@ int spect_subset_sensitivity(spect_plan_t p, float* asum, const int32_t* index, 
   const int* vi;
   STATUS_TRY(stage_index(p, index, nindex, st, &vi));
   return backward(p, asum, p->d_ones, vi, nindex, st, 1, nullptr);
+}
+
+unsigned long long spect_kernel_launches(void) { return g_launches.load(); }
+
+int spect_plan_profile(spect_plan_t p, int on) {
+  if (!p) return fail(SPECT_ERR_ARG, "null plan");
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->prof.reset();
+  p->prof.on = on != 0;
+  return SPECT_OK;
+}
+
+int spect_plan_kernel_times(spect_plan_t p, double ms[8], long long counts[8]) {
+  if (!p || !ms || !counts) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  p->prof.drain();
+  for (int k = 0; k < K_KINDS; ++k) {
+    ms[k] = p->prof.ms[k];
+    counts[k] = p->prof.n[k];
+  }
+  return SPECT_OK;
 }
 
 int spect_psf_gauss(float* psf, int ny, int px, int pz, const double* fwhm_x, const double* fwhm_z) {
