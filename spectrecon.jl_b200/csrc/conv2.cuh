@@ -1,0 +1,572 @@
+// conv2.cuh -- depth-dependent PSF convolution kernels (sm_100a), templated
+// on the register counts RX = Npx/CX and RZ = Npz/CZ of the two FFT axes.
+//
+// Reference semantics: fft_conv! / fft_conv_adj! (src/fft_convolve.jl:33-130)
+// on planes replicate-padded (adjoint: zero-padded then folded) to
+// Npx x Npz = Power2(nx+px-1) x Power2(nz+pz-1) (src/helper.jl:8-12), with
+// the depth sum of project! (src/project.jl:127-130).
+//
+// Data layout on chip, per CTA:
+//   B[x][c]  (shared memory when it fits, else a per-CTA global slab), nx
+//            rows of QS = Q+1 complex: the z-spectrum of each image row at the
+//            Q = Npz/2 stored z-frequencies.  Column c holds kz = k1 +
+//            RZ*brev(2*(c mod CZ/2)) with k1 = c / (CZ/2) (the scrambled order
+//            of the z transform, even lanes), except column 0 which packs the
+//            two real columns kz = 0 (.x) and kz = Npz/2 (.y).  The same
+//            memory first holds the real plane, row x at floats [2*QS*x, +nz).
+//   x-spectra live in registers in the scrambled order of fft_reg.cuh; the
+//   plan stores the PSF spectra in exactly that order:
+//     Hs[set][y][c][k1*CX + l]  = H(kx, kz(c)) / (Npx*Npz),  c = 1..Q-1
+//     Hs[set][y][0][..] = (H(kx,0) + H(kx,Npz/2))/2, Hs[set][y][Q][..] = (H(kx,0) - H(kx,Npz/2))/2
+//   so that for the packed column Y' = alpha*Y + beta*conj(Y(-kx)).
+// Forward: the x-spectra of all planes of a depth chunk are multiplied by
+// their PSF spectra and summed in registers (one inverse transform per chunk,
+// not per plane).  Adjoint: the view spectrum is computed once (k_vspec2) and
+// held in registers across the chunk.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_reg.cuh"
+
+namespace spect {
+
+constexpr int kConvThreads = 512;
+constexpr int kConvWarps = kConvThreads / 32;
+
+struct ConvGeom {
+  int nx, ny, nz;
+  int Npx, Npz, logNpx, logNpz;
+  int padup, padleft;
+  int hx, hz;        // PSF half widths (px-1)/2, (pz-1)/2: extent of the folds
+  int Q, QS;         // stored z-columns (max(1, Npz/2)) and B row stride (Q+1)
+  int CX, logCX;     // lanes per x transform
+  int CZ, logCZ;     // lanes per z transform
+};
+
+struct Conv2Args {
+  ConvGeom g;
+  const float* P;       // forward input planes  [nv][ny][nz][nx]
+  float* T;             // adjoint output planes [nv][ny][nz][nx]
+  const float* Hs;      // [nset][ny][Q+1][Npx]
+  const int* vidx;      // [nv] plan view of each slot
+  const int* viewset;   // [nview] spectrum set of each view
+  const float2* Vs;     // adjoint input  [nv][Q][Npx] scrambled view spectra
+  float2* VsOut;        // k_vspec2 output
+  const float* views;   // k_vspec2 input [nv][nz][nx]
+  int nv, chunkY, nchunks;
+  float* part;          // forward output [nv][nchunks][nz][nx]
+  float2* gB;           // per-CTA B slabs (nx*QS) when B is not in shared memory
+  float2* gacc;         // per-CTA spectra slabs (Q*Npx) when they are not in registers
+  const float2* tw;     // twiddles exp(-2 pi i m / SPECT_TW_N)
+  int bsmem;
+};
+
+struct Lanes {
+  int l, g, gbase;  // lane in group, group in warp, first lane of group
+};
+__device__ __forceinline__ Lanes lanes_of(int lane, int logC) {
+  Lanes L;
+  L.l = lane & ((1 << logC) - 1);
+  L.g = lane >> logC;
+  L.gbase = L.g << logC;
+  return L;
+}
+
+__device__ __forceinline__ float2* conv_setup(const Conv2Args& a, float2** twp) {
+  extern __shared__ float4 smem4[];
+  float2* tw = reinterpret_cast<float2*>(smem4);
+  for (int k = threadIdx.x; k < SPECT_TW_N; k += blockDim.x) tw[k] = a.tw[k];
+  *twp = tw;
+  __syncthreads();
+  if (a.bsmem) return tw + SPECT_TW_N;
+  return a.gB + (size_t)blockIdx.x * a.g.nx * a.g.QS;
+}
+
+// (x, z) walk of a thread over an nz x nx plane in steps of blockDim.x
+struct PlaneWalk {
+  int x0, z0, dx, dz;
+  __device__ __forceinline__ PlaneWalk(int nx) {
+    z0 = threadIdx.x / nx;
+    x0 = threadIdx.x - z0 * nx;
+    dz = blockDim.x / nx;
+    dx = blockDim.x - dz * nx;
+  }
+};
+
+// real nz x nx plane (x fastest) -> real rows of B
+__device__ __forceinline__ void load_plane(const ConvGeom& g, const PlaneWalk& W, float2* B,
+                                           const float* __restrict__ src) {
+  float* Bf = reinterpret_cast<float*>(B);
+  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
+  int x = W.x0, z = W.z0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    Bf[x * rs + z] = __ldg(src + k);
+    x += W.dx;
+    z += W.dz;
+    if (x >= nx) {
+      x -= nx;
+      ++z;
+    }
+  }
+}
+
+// real rows of B -> nz x nx plane (x fastest) in global memory
+__device__ __forceinline__ void store_plane(const ConvGeom& g, const PlaneWalk& W, const float2* B,
+                                            float* __restrict__ dst) {
+  const float* Bf = reinterpret_cast<const float*>(B);
+  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
+  int x = W.x0, z = W.z0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    dst[k] = Bf[x * rs + z];
+    x += W.dx;
+    z += W.dz;
+    if (x >= nx) {
+      x -= nx;
+      ++z;
+    }
+  }
+}
+
+// Per-lane index tables, computed once per kernel.
+//   zrd[r]  z source of register r for the forward z transform (clamped, or
+//           -1 outside the image when zero padding)
+//   zg[k1]  stored-column gather code for the inverse z transform:
+//           (c << 2) | mode, mode 0 b[c], 1 conj(b[c]), 2 real b[c].x, 3 real b[c].y
+//   xrd[r]  B row offset (x * QS) read by register r of the x transform
+//           (clamped, or -1 outside the image when zero padding)
+//   xwr[r]  B row offset written by register r after the inverse x transform
+//           (-1 when cropped away)
+template <int RX, int RZ>
+struct LaneTables {
+  int zrd[RZ], zg[RZ], xrd[RX], xwr[RX];
+  // READ: zrd, xrd (forward transforms); WRITE: zg, xwr (inverse transforms)
+  __device__ __forceinline__ void init(const ConvGeom& g, int lane, bool zeropad, bool read = true,
+                                       bool write = true) {
+    const int lz = lane & (g.CZ - 1), lx = lane & (g.CX - 1);
+    const int CZ = g.CZ, half = CZ >> 1;
+    if (read) {
+#pragma unroll
+      for (int r = 0; r < RZ; ++r) {
+        int zc = lz + CZ * r - g.padleft;
+        if (zeropad) zrd[r] = ((unsigned)zc < (unsigned)g.nz) ? zc : -1;
+        else zrd[r] = min(max(zc, 0), g.nz - 1);
+      }
+#pragma unroll
+      for (int r = 0; r < RX; ++r) {
+        int x = lx + g.CX * r - g.padup;
+        if (zeropad) xrd[r] = ((unsigned)x < (unsigned)g.nx) ? x * g.QS : -1;
+        else xrd[r] = min(max(x, 0), g.nx - 1) * g.QS;
+      }
+    }
+    if (!write) return;
+#pragma unroll
+    for (int k1 = 0; k1 < RZ; ++k1) {
+      int code;
+      if (CZ == 1) {
+        code = 2;
+      } else if ((lz & 1) == 0) {
+        const int c = k1 * half + (lz >> 1);
+        code = (c == 0) ? 2 : (c << 2);
+      } else if (k1 == 0 && lz == 1) {
+        code = 3;
+      } else {
+        int lp, rp;
+        if (k1 > 0) {
+          lp = lz ^ (CZ - 1);
+          rp = RZ - k1;
+        } else {
+          lp = brev_rt((CZ - brev_rt(lz, g.logCZ)) & (CZ - 1), g.logCZ);
+          rp = 0;
+        }
+        code = ((rp * half + (lp >> 1)) << 2) | 1;
+      }
+      zg[k1] = code;
+    }
+#pragma unroll
+    for (int r = 0; r < RX; ++r) {
+      int x = lx + g.CX * r - g.padup;
+      xwr[r] = ((unsigned)x < (unsigned)g.nx) ? x * g.QS : -1;
+    }
+  }
+};
+
+// z transform of row pairs (x0, x0+1), in place in B: real rows -> stored
+// columns.  ZEROPAD: zero padding (adjoint) instead of replication.
+template <int RZ, bool ZEROPAD>
+__device__ __forceinline__ void zfft_rows_fwd(const ConvGeom& g, float2* B, const float2* __restrict__ tw, int warp,
+                                              int lane, const int (&zrd)[RZ]) {
+  const Lanes L = lanes_of(lane, g.logCZ);
+  const int CZ = g.CZ, GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
+  const int npairs = g.nx >> 1, iters = (npairs + units - 1) / units;
+  float* Bf = reinterpret_cast<float*>(B);
+  const int rs = 2 * g.QS, QS = g.QS, half = CZ >> 1;
+  for (int it = 0; it < iters; ++it) {
+    const int rp = it * units + warp * GZ + L.g;
+    const bool active = rp < npairs;
+    const int x0 = 2 * min(rp, npairs - 1);
+    const float* r0 = Bf + x0 * rs;
+    const float* r1 = r0 + rs;
+    float2 v[RZ];
+#pragma unroll
+    for (int r = 0; r < RZ; ++r) {
+      const int zc = zrd[r];
+      if (ZEROPAD) v[r] = (zc >= 0) ? make_float2(r0[zc], r1[zc]) : make_float2(0.f, 0.f);
+      else v[r] = make_float2(r0[zc], r1[zc]);
+    }
+    __syncwarp();
+    fft_fwd<RZ>(v, L.l, g.logCZ, g.logNpz, tw);
+    // partners: register k1 <-> RZ-k1 in lane l ^ (CZ-1); register 0 via brev
+    float2 p[RZ];
+    p[0] = shfl2(v[0], L.gbase + brev_rt((CZ - brev_rt(L.l, g.logCZ)) & (CZ - 1), g.logCZ));
+#pragma unroll
+    for (int k1 = 1; k1 < RZ; ++k1) p[k1] = shfl_xor2(v[RZ - k1], CZ - 1);
+    if (active) {
+      float2* b0 = B + x0 * QS;
+      float2* b1 = b0 + QS;
+      float* f0 = reinterpret_cast<float*>(b0);
+      float* f1 = reinterpret_cast<float*>(b1);
+#pragma unroll
+      for (int k1 = 0; k1 < RZ; ++k1) {
+        // two real rows from one complex transform
+        float2 A = make_float2(0.5f * (v[k1].x + p[k1].x), 0.5f * (v[k1].y - p[k1].y));
+        float2 Bb = make_float2(0.5f * (v[k1].y + p[k1].y), 0.5f * (p[k1].x - v[k1].x));
+        if (CZ == 1) {
+          b0[0] = make_float2(A.x, 0.f);
+          b1[0] = make_float2(Bb.x, 0.f);
+        } else if ((L.l & 1) == 0) {
+          const int c = k1 * half + (L.l >> 1);
+          if (c == 0) {
+            f0[0] = A.x;
+            f1[0] = Bb.x;
+          } else {
+            b0[c] = A;
+            b1[c] = Bb;
+          }
+        } else if (k1 == 0 && L.l == 1) {  // Nyquist, packed in column 0
+          f0[1] = A.x;
+          f1[1] = Bb.x;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// Hermitian z-spectrum of the row pair from the stored columns, in the
+// scrambled input order of fft_inv: v = Z0 + i Z1 (gather codes: LaneTables::zg)
+template <int RZ>
+__device__ __forceinline__ void gather_zspec(const float2* b0, const float2* b1, const int (&zg)[RZ],
+                                             float2 (&v)[RZ]) {
+#pragma unroll
+  for (int k1 = 0; k1 < RZ; ++k1) {
+    const int code = zg[k1], c = code >> 2, mode = code & 3;
+    float2 a = b0[c], b = b1[c];
+    if (mode == 1) {
+      a.y = -a.y;
+      b.y = -b.y;
+    } else if (mode >= 2) {
+      const bool hiq = mode == 3;
+      a = make_float2(hiq ? a.y : a.x, 0.f);
+      b = make_float2(hiq ? b.y : b.x, 0.f);
+    }
+    v[k1] = make_float2(a.x - b.y, a.y + b.x);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ float2 group_sum(float2 s, int logC) {
+  for (int q = 0; q < logC; ++q) s = cadd(s, shfl_xor2(s, 1 << q));
+  return s;
+}
+
+// inverse z transform of row pairs: stored columns -> real rows (in place).
+// FOLD: adjoint of the replicate padding: the padded samples are summed into
+// the edge samples.  Of the padded samples only the hz next to the image can
+// be non-zero (zero-padded input, PSF half width hz, no wrap-around since the
+// pads are >= hz), so only those are summed; the rest hold FFT round-off.
+template <int RZ, bool FOLD>
+__device__ __forceinline__ void zfft_rows_inv(const ConvGeom& g, float2* B, const float2* __restrict__ tw, int warp,
+                                              int lane, const int (&zg)[RZ]) {
+  const Lanes L = lanes_of(lane, g.logCZ);
+  const int CZ = g.CZ, GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
+  const int npairs = g.nx >> 1, iters = (npairs + units - 1) / units;
+  float* Bf = reinterpret_cast<float*>(B);
+  const int rs = 2 * g.QS, QS = g.QS;
+  for (int it = 0; it < iters; ++it) {
+    const int rp = it * units + warp * GZ + L.g;
+    const bool active = rp < npairs;
+    const int x0 = 2 * min(rp, npairs - 1);
+    float2 v[RZ];
+    gather_zspec<RZ>(B + x0 * QS, B + (x0 + 1) * QS, zg, v);
+    __syncwarp();
+    fft_inv<RZ>(v, L.l, g.logCZ, g.logNpz, tw);
+    float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
+    if (FOLD) {
+#pragma unroll
+      for (int r = 0; r < RZ; ++r) {
+        int z = L.l + CZ * r - g.padleft;
+        if (z < 0 && z >= -g.hz) lo = cadd(lo, v[r]);
+        else if (z >= g.nz && z < g.nz + g.hz) hi = cadd(hi, v[r]);
+      }
+      lo = group_sum<RZ>(lo, g.logCZ);
+      hi = group_sum<RZ>(hi, g.logCZ);
+    }
+    if (active) {
+      float* r0 = Bf + x0 * rs;
+      float* r1 = r0 + rs;
+#pragma unroll
+      for (int r = 0; r < RZ; ++r) {
+        int z = L.l + CZ * r - g.padleft;
+        if ((unsigned)z < (unsigned)g.nz) {
+          float2 w = v[r];
+          if (FOLD) {
+            if (z == 0) w = cadd(w, lo);
+            if (z == g.nz - 1) w = cadd(w, hi);
+          }
+          r0[z] = w.x;
+          r1[z] = w.y;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// point-wise product with the plane's PSF spectrum (scrambled order).
+// PACKED (warp-uniform): this warp holds column 0 in group 0.
+template <int RX>
+__device__ __forceinline__ void apply_psf(float2 (&v)[RX], const float* __restrict__ h, const float* __restrict__ hb,
+                                          const Lanes& L, int logCX, bool packed_warp, bool col0) {
+  const int CX = 1 << logCX;
+  if (packed_warp) {
+    // Y' = alpha Y + beta conj(Y(-k)); registers k1 and RX-k1 are partners
+    const int src0 = L.gbase + brev_rt((CX - brev_rt(L.l, logCX)) & (CX - 1), logCX);
+    const float2 p0 = shfl2(v[0], src0);
+    if (col0) v[0] = make_float2(__ldg(h) * v[0].x + __ldg(hb) * p0.x, __ldg(h) * v[0].y - __ldg(hb) * p0.y);
+#pragma unroll
+    for (int k1 = 1; k1 <= RX / 2; ++k1) {
+      const int k2 = RX - k1;
+      const float2 pa = shfl_xor2(v[k2], CX - 1);  // partner of register k1
+      const float2 pb = shfl_xor2(v[k1], CX - 1);  // partner of register k2
+      if (col0) {
+        float al = __ldg(h + k1 * CX), be = __ldg(hb + k1 * CX);
+        v[k1] = make_float2(al * v[k1].x + be * pa.x, al * v[k1].y - be * pa.y);
+        if (k2 != k1) {
+          al = __ldg(h + k2 * CX);
+          be = __ldg(hb + k2 * CX);
+          v[k2] = make_float2(al * v[k2].x + be * pb.x, al * v[k2].y - be * pb.y);
+        }
+      }
+    }
+    if (col0) return;
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < RX; ++k1) v[k1] = cscale(v[k1], __ldg(h + k1 * CX));
+}
+
+// ------------------------------------------------------------------------
+// forward: persistent over items (slot, depth chunk)
+template <int RX, int RZ, bool REGACC>
+__global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
+  const ConvGeom& g = a.g;
+  float2* tw;
+  float2* B = conv_setup(a, &tw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const Lanes L = lanes_of(lane, g.logCX);
+  const int CX = g.CX, GX = 32 >> g.logCX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
+  const int JC = (Q + units - 1) / units;
+  constexpr int JM = RZ > 1 ? RZ : 1;
+  const int nitems = a.nv * a.nchunks;
+  float2 acc[REGACC ? JM : 1][RX];
+  float2* gacc = a.gacc + (size_t)blockIdx.x * Q * Npx;
+  const PlaneWalk W(g.nx);
+  LaneTables<RX, RZ> T;
+  T.init(g, lane, false, true, false);
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int slot = item / a.nchunks, ch = item - slot * a.nchunks;
+    const int y0 = ch * a.chunkY, y1 = min(g.ny, y0 + a.chunkY);
+    const float* Pv = a.P + (size_t)slot * g.ny * g.nz * g.nx;
+    const float* Hv = a.Hs + (size_t)a.viewset[a.vidx[slot]] * g.ny * (Q + 1) * Npx;
+    for (int y = y0; y < y1; ++y) {
+      __syncthreads();
+      load_plane(g, W, B, Pv + (size_t)y * g.nz * g.nx);
+      __syncthreads();
+      zfft_rows_fwd<RZ, false>(g, B, tw, warp, lane, T.zrd);
+      __syncthreads();
+      const float* Hy = Hv + (size_t)y * (Q + 1) * Npx;
+#pragma unroll
+      for (int j = 0; j < JM; ++j) {
+        if (j < JC) {
+          const int c = j * units + warp * GX + L.g;
+          const bool active = c < Q;
+          const int cc = min(c, Q - 1);
+          float2 v[RX];
+#pragma unroll
+          for (int r = 0; r < RX; ++r) v[r] = B[T.xrd[r] + cc];
+          fft_fwd<RX>(v, L.l, g.logCX, g.logNpx, tw);
+          apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX,
+                        j == 0 && warp == 0, cc == 0);
+          if (active) {
+            if (REGACC) {
+#pragma unroll
+              for (int k1 = 0; k1 < RX; ++k1) acc[REGACC ? j : 0][k1] = (y == y0) ? v[k1] : cadd(acc[REGACC ? j : 0][k1], v[k1]);
+            } else {
+              float2* ga = gacc + (size_t)c * Npx + L.l;
+#pragma unroll
+              for (int k1 = 0; k1 < RX; ++k1) ga[k1 * CX] = (y == y0) ? v[k1] : cadd(ga[k1 * CX], v[k1]);
+            }
+          }
+        }
+      }
+    }
+    // chunk end: inverse x transform, crop to nx rows
+    __syncthreads();
+    LaneTables<RX, RZ> TW;
+    TW.init(g, lane, false, false, true);
+#pragma unroll
+    for (int j = 0; j < JM; ++j) {
+      if (j < JC) {
+        const int c = j * units + warp * GX + L.g;
+        const bool active = c < Q;
+        float2 v[RX];
+        if (REGACC) {
+#pragma unroll
+          for (int k1 = 0; k1 < RX; ++k1) v[k1] = acc[REGACC ? j : 0][k1];
+        } else {
+          const float2* ga = gacc + (size_t)min(c, Q - 1) * Npx + L.l;
+#pragma unroll
+          for (int k1 = 0; k1 < RX; ++k1) v[k1] = ga[k1 * CX];
+        }
+        fft_inv<RX>(v, L.l, g.logCX, g.logNpx, tw);
+        if (active) {
+#pragma unroll
+          for (int r = 0; r < RX; ++r)
+            if (TW.xwr[r] >= 0) B[TW.xwr[r] + c] = v[r];
+        }
+      }
+    }
+    __syncthreads();
+    zfft_rows_inv<RZ, false>(g, B, tw, warp, lane, TW.zg);
+    __syncthreads();
+    store_plane(g, W, B, a.part + ((size_t)slot * a.nchunks + ch) * g.nz * g.nx);
+  }
+}
+
+// ------------------------------------------------------------------------
+// scrambled spectrum of each zero-padded view: VsOut[slot][c][k1*CX + l]
+template <int RX, int RZ>
+__global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
+  const ConvGeom& g = a.g;
+  float2* tw;
+  float2* B = conv_setup(a, &tw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const Lanes L = lanes_of(lane, g.logCX);
+  const int CX = g.CX, GX = 32 >> g.logCX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
+  const int iters = (Q + units - 1) / units;
+  const PlaneWalk W(g.nx);
+  LaneTables<RX, RZ> T;
+  T.init(g, lane, true);
+  for (int slot = blockIdx.x; slot < a.nv; slot += gridDim.x) {
+    __syncthreads();
+    load_plane(g, W, B, a.views + (size_t)slot * g.nz * g.nx);
+    __syncthreads();
+    zfft_rows_fwd<RZ, true>(g, B, tw, warp, lane, T.zrd);
+    __syncthreads();
+    for (int it = 0; it < iters; ++it) {
+      const int c = it * units + warp * GX + L.g;
+      const int cc = min(c, Q - 1);
+      float2 v[RX];
+#pragma unroll
+      for (int r = 0; r < RX; ++r) v[r] = (T.xrd[r] >= 0) ? B[T.xrd[r] + cc] : make_float2(0.f, 0.f);
+      fft_fwd<RX>(v, L.l, g.logCX, g.logNpx, tw);
+      if (c < Q) {
+        float2* o = a.VsOut + ((size_t)slot * Q + c) * Npx + L.l;
+#pragma unroll
+        for (int k1 = 0; k1 < RX; ++k1) o[k1 * CX] = v[k1];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// adjoint: persistent over items (slot, depth chunk); T[slot][y][z][x]
+template <int RX, int RZ, bool REGACC>
+__global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
+  const ConvGeom& g = a.g;
+  float2* tw;
+  float2* B = conv_setup(a, &tw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const Lanes L = lanes_of(lane, g.logCX);
+  const int CX = g.CX, GX = 32 >> g.logCX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
+  const int JC = (Q + units - 1) / units;
+  constexpr int JM = RZ > 1 ? RZ : 1;
+  const int nitems = a.nv * a.nchunks;
+  float2 vs[REGACC ? JM : 1][RX];
+  const PlaneWalk W(g.nx);
+  LaneTables<RX, RZ> T;
+  T.init(g, lane, false);
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int slot = item / a.nchunks, ch = item - slot * a.nchunks;
+    const int y0 = ch * a.chunkY, y1 = min(g.ny, y0 + a.chunkY);
+    const float* Hv = a.Hs + (size_t)a.viewset[a.vidx[slot]] * g.ny * (Q + 1) * Npx;
+    const float2* Vsl = a.Vs + (size_t)slot * Q * Npx;
+    if (REGACC) {
+#pragma unroll
+      for (int j = 0; j < JM; ++j) {
+        if (j < JC) {
+          const int cc = min(j * units + warp * GX + L.g, Q - 1);
+#pragma unroll
+          for (int k1 = 0; k1 < RX; ++k1) vs[REGACC ? j : 0][k1] = Vsl[(size_t)cc * Npx + L.l + k1 * CX];
+        }
+      }
+    }
+    for (int y = y0; y < y1; ++y) {
+      const float* Hy = Hv + (size_t)y * (Q + 1) * Npx;
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < JM; ++j) {
+        if (j < JC) {
+          const int c = j * units + warp * GX + L.g;
+          const bool active = c < Q;
+          const int cc = min(c, Q - 1);
+          float2 v[RX];
+#pragma unroll
+          for (int k1 = 0; k1 < RX; ++k1)
+            v[k1] = REGACC ? vs[REGACC ? j : 0][k1] : Vsl[(size_t)cc * Npx + L.l + k1 * CX];
+          apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX,
+                        j == 0 && warp == 0, cc == 0);
+          fft_inv<RX>(v, L.l, g.logCX, g.logNpx, tw);
+          // adjoint of the replicate padding along x
+          float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
+#pragma unroll
+          for (int r = 0; r < RX; ++r) {
+            int x = L.l + CX * r - g.padup;
+            if (x < 0 && x >= -g.hx) lo = cadd(lo, v[r]);
+            else if (x >= g.nx && x < g.nx + g.hx) hi = cadd(hi, v[r]);
+          }
+          lo = group_sum<RX>(lo, g.logCX);
+          hi = group_sum<RX>(hi, g.logCX);
+          if (active) {
+#pragma unroll
+            for (int r = 0; r < RX; ++r) {
+              const int off = T.xwr[r];
+              if (off >= 0) {
+                float2 w = v[r];
+                if (off == 0) w = cadd(w, lo);
+                if (off == (g.nx - 1) * g.QS) w = cadd(w, hi);
+                B[off + c] = w;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+      zfft_rows_inv<RZ, true>(g, B, tw, warp, lane, T.zg);
+      __syncthreads();
+      store_plane(g, W, B, a.T + ((size_t)slot * g.ny + y) * g.nz * g.nx);
+    }
+  }
+}
+
+}  // namespace spect

@@ -8,14 +8,15 @@
 //
 // Device memory layout (HBM), all float32 unless noted:
 //   mumap   [nz][ny][nx]                 uploaded once per plan
-//   H       [nset][ny][Hz][Npx]          real PSF spectra, one set per distinct
-//                                        psfs[:,:,:,v] (views with identical
-//                                        PSF stacks share a set)
+//   Hs      [nset][ny][Q+1][Npx]         real PSF spectra / (Npx*Npz) in the
+//                                        scrambled orders of conv2.cuh, one set
+//                                        per distinct psfs[:,:,:,v] (views with
+//                                        identical PSF stacks share a set)
 //   P / T   [gmax][ny][nz][nx]           rotated+attenuated planes (forward) /
 //                                        adjoint-convolved planes (adjoint) of
 //                                        one group of views
 //   part    [gmax][nchunk][nz][nx]       per depth-chunk partial views
-//   Vhat    [gmax][Hz][Npx] complex      spectra of the views (adjoint)
+//   Vs      [gmax][Q][Npx] complex       spectra of the views (adjoint)
 //   imgpart [nsplit][nz][ny][nx]         per view-split partial images
 #include <cuda_runtime.h>
 
@@ -29,9 +30,23 @@
 #include <vector>
 
 #include "../../include/spect_gpu.h"
+#include "conv2.cuh"
 #include "spect_kernels.cuh"
 
 using namespace spect;
+
+namespace spect {
+// per-RX instantiation units (conv_inst.cu)
+#define SPECT_DECL_RX(n)                                                                                   \
+  cudaError_t conv2_launch_rx##n(int kind, int RZ, int grid, size_t smem, cudaStream_t st, const Conv2Args& a); \
+  cudaError_t conv2_setup_rx##n(int RZ, size_t smem, int* occ);
+SPECT_DECL_RX(1)
+SPECT_DECL_RX(2)
+SPECT_DECL_RX(4)
+SPECT_DECL_RX(8)
+SPECT_DECL_RX(16)
+#undef SPECT_DECL_RX
+}  // namespace spect
 
 namespace {
 
@@ -149,10 +164,10 @@ struct spect_plan_s {
   int gmax = 1, nchunk_max = 16;
   float* d_P = nullptr;
   float* d_part = nullptr;
-  float2* d_Vhat = nullptr;
+  float2* d_Vs = nullptr;
   float* d_imgpart = nullptr;
   float2* d_gB = nullptr;
-  float* d_gacc = nullptr;
+  float2* d_gacc = nullptr;
   float* d_gscr_adj = nullptr;
   // EM scratch (lazily allocated)
   float* d_views_tmp = nullptr;  // [nview][nz][nx]
@@ -164,7 +179,9 @@ struct spect_plan_s {
   float* d_io_img = nullptr;   // [2][N]
   float* d_io_views = nullptr; // [3][nview][nz][nx]
   // launch configuration
-  int conv_grid = 148, conv_bsmem = 1, conv_asmem = 1;
+  ConvGeom cg;
+  int RX = 1, RZ = 1;
+  int conv_grid = 148, conv_bsmem = 1;
   size_t conv_smem = 0;
   int rotf_vpb = 1, rotf_smem_ok = 1;
   size_t rotf_smem = 0;
@@ -193,7 +210,7 @@ int dalloc(spect_plan_s* p, T** ptr, size_t count) {
 
 void free_plan(spect_plan_s* p) {
   void* ptrs[] = {p->d_mumap, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
-                  p->d_idx,   p->d_P,     p->d_part,     p->d_Vhat,      p->d_imgpart,    p->d_gB,
+                  p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag,
                   p->d_io_img, p->d_io_views};
   for (void* q : ptrs)
@@ -236,34 +253,43 @@ int configure(spect_plan_s* p) {
   p->max_smem = (size_t)optin;
   const Geom& g = p->g;
   // ---- convolution kernels
-  const int maxN = std::max(g.Npx, g.Npz);
-  size_t base = sizeof(float2) * (SPECT_TW_N + (size_t)kConvWarps * maxN);
-  size_t Bb = sizeof(float2) * (size_t)g.nx * g.Hz;
-  size_t Ab = sizeof(float) * (size_t)g.nz * (g.nx + 2);
-  if (base + Bb + Ab <= p->max_smem) {
-    p->conv_bsmem = 1;
-    p->conv_asmem = 1;
-    p->conv_smem = base + Bb + Ab;
-  } else if (base + Bb <= p->max_smem) {
-    p->conv_bsmem = 1;
-    p->conv_asmem = 0;
-    p->conv_smem = base + Bb;
-  } else {
-    p->conv_bsmem = 0;
-    p->conv_asmem = (base + Ab <= p->max_smem) ? 1 : 0;
-    p->conv_smem = base + (p->conv_asmem ? Ab : 0);
+  ConvGeom& cg = p->cg;
+  cg.nx = g.nx;
+  cg.ny = g.ny;
+  cg.nz = g.nz;
+  cg.Npx = g.Npx;
+  cg.Npz = g.Npz;
+  cg.logNpx = g.logNpx;
+  cg.logNpz = g.logNpz;
+  cg.padup = g.padup;
+  cg.padleft = g.padleft;
+  cg.hx = (p->px - 1) / 2;
+  cg.hz = (p->pz - 1) / 2;
+  cg.Q = std::max(1, g.Npz / 2);
+  cg.QS = cg.Q + 1;
+  cg.CX = std::min(32, g.Npx);
+  cg.logCX = ilog2(cg.CX);
+  cg.CZ = std::min(32, g.Npz);
+  cg.logCZ = ilog2(cg.CZ);
+  p->RX = g.Npx / cg.CX;
+  p->RZ = g.Npz / cg.CZ;
+  size_t base = sizeof(float2) * SPECT_TW_N;
+  size_t Bb = sizeof(float2) * (size_t)g.nx * cg.QS;
+  p->conv_bsmem = (base + Bb <= p->max_smem) ? 1 : 0;
+  p->conv_smem = base + (p->conv_bsmem ? Bb : 0);
+  int occ = 1;
+  cudaError_t ce = cudaErrorInvalidValue;
+  switch (p->RX) {
+    case 1: ce = conv2_setup_rx1(p->RZ, p->conv_smem, &occ); break;
+    case 2: ce = conv2_setup_rx2(p->RZ, p->conv_smem, &occ); break;
+    case 4: ce = conv2_setup_rx4(p->RZ, p->conv_smem, &occ); break;
+    case 8: ce = conv2_setup_rx8(p->RZ, p->conv_smem, &occ); break;
+    case 16: ce = conv2_setup_rx16(p->RZ, p->conv_smem, &occ); break;
   }
-  const void* convk[] = {(const void*)k_conv_fwd, (const void*)k_conv_adj, (const void*)k_vspec};
-  int occ = 8;
-  for (const void* k : convk) {
-    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->conv_smem));
-    int o = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, kConvThreads, p->conv_smem));
-    occ = std::min(occ, std::max(o, 1));
-  }
-  p->conv_grid = p->sm_count * occ;
-  if (!p->conv_bsmem) STATUS_TRY(dalloc(p, &p->d_gB, (size_t)g.nx * g.Hz * p->conv_grid));
-  if (!p->conv_asmem) STATUS_TRY(dalloc(p, &p->d_gacc, (size_t)g.nz * (g.nx + 2) * p->conv_grid));
+  if (ce != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string("conv kernel setup: ") + cudaGetErrorString(ce));
+  p->conv_grid = p->sm_count * std::max(occ, 1);
+  if (!p->conv_bsmem) STATUS_TRY(dalloc(p, &p->d_gB, (size_t)g.nx * cg.QS * p->conv_grid));
+  if (p->RX * p->RZ > 32) STATUS_TRY(dalloc(p, &p->d_gacc, (size_t)cg.Q * g.Npx * p->conv_grid));
   // ---- forward rotation
   p->rotf_vpb = std::max(1, std::min(8, 512 / g.nx));
   size_t slice = (size_t)g.nx * g.ny;
@@ -296,18 +322,28 @@ void chunking(const spect_plan_s* p, int nv, int* chunkY, int* nchunks) {
   *nchunks = cdiv(p->ny, cy);
 }
 
-ConvArgs conv_args(const spect_plan_s* p) {
-  ConvArgs a;
+Conv2Args conv_args(const spect_plan_s* p) {
+  Conv2Args a;
   std::memset(&a, 0, sizeof(a));
-  a.g = p->g;
-  a.H = p->d_H;
+  a.g = p->cg;
+  a.Hs = p->d_H;
   a.viewset = p->d_viewset;
   a.gB = p->d_gB;
   a.gacc = p->d_gacc;
   a.tw = p->d_tw;
   a.bsmem = p->conv_bsmem;
-  a.asmem = p->conv_asmem;
   return a;
+}
+
+cudaError_t conv_launch(const spect_plan_s* p, int kind, int grid, cudaStream_t st, const Conv2Args& a) {
+  switch (p->RX) {
+    case 1: return conv2_launch_rx1(kind, p->RZ, grid, p->conv_smem, st, a);
+    case 2: return conv2_launch_rx2(kind, p->RZ, grid, p->conv_smem, st, a);
+    case 4: return conv2_launch_rx4(kind, p->RZ, grid, p->conv_smem, st, a);
+    case 8: return conv2_launch_rx8(kind, p->RZ, grid, p->conv_smem, st, a);
+    case 16: return conv2_launch_rx16(kind, p->RZ, grid, p->conv_smem, st, a);
+  }
+  return cudaErrorInvalidValue;
 }
 
 // forward projection of nidx views (device index list vidx) into views;
@@ -328,7 +364,7 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
                                                                                          p->d_rot, vi, nv, p->d_P);
            else k_rot_fwd<false><<<grid, g.nx * vpb, 0, st>>>(g, image, p->d_mumap, p->d_rot, vi, nv, p->d_P));
     // FFT convolution + depth sum -> part
-    ConvArgs a = conv_args(p);
+    Conv2Args a = conv_args(p);
     int cy, nc;
     chunking(p, nv, &cy, &nc);
     a.P = p->d_P;
@@ -338,7 +374,7 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
     a.nchunks = nc;
     a.part = p->d_part;
     int gridc = std::min(p->conv_grid, nv * nc);
-    LAUNCH(p, K_CONV_FWD, st, "k_conv_fwd", k_conv_fwd<<<gridc, kConvThreads, p->conv_smem, st>>>(a));
+    LAUNCH(p, K_CONV_FWD, st, "k_conv_fwd", conv_launch(p, 0, gridc, st, a));
     // chunk sum (+ EM ratio) -> views
     size_t n = (size_t)nv * p->nxz;
     int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16);
@@ -362,20 +398,19 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
   for (int g0 = 0; g0 < nidx; g0 += p->gmax) {
     const int nv = std::min(p->gmax, nidx - g0);
     const int* vi = vidx + g0;
-    ConvArgs a = conv_args(p);
+    Conv2Args a = conv_args(p);
     a.views = views + (size_t)g0 * p->nxz;
-    a.VhatOut = p->d_Vhat;
+    a.VsOut = p->d_Vs;
     a.nv = nv;
     a.vidx = vi;
-    LAUNCH(p, K_VSPEC, st, "k_vspec", k_vspec<<<std::min(p->conv_grid, nv), kConvThreads, p->conv_smem, st>>>(a));
+    LAUNCH(p, K_VSPEC, st, "k_vspec", conv_launch(p, 2, std::min(p->conv_grid, nv), st, a));
     int cy, nc;
     chunking(p, nv, &cy, &nc);
-    a.Vhat = p->d_Vhat;
+    a.Vs = p->d_Vs;
     a.T = p->d_P;
     a.chunkY = cy;
     a.nchunks = nc;
-    LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj",
-           k_conv_adj<<<std::min(p->conv_grid, nv * nc), kConvThreads, p->conv_smem, st>>>(a));
+    LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj", conv_launch(p, 1, std::min(p->conv_grid, nv * nc), st, a));
     dim3 grid(g.nz, nsplit);
     LAUNCH(p, K_ROT_ADJ, st, "k_rot_adj",
            k_rot_adj<<<grid, kRotAdjThreads, p->rota_smem_ok ? p->rota_smem : 0, st>>>(
@@ -589,10 +624,10 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
   if ((st = dalloc(p, &p->d_mumap, p->N)) || (st = dalloc(p, &p->d_rot, nview)) ||
       (st = dalloc(p, &p->d_viewset, nview)) || (st = dalloc(p, &p->d_tw, SPECT_TW_N)) ||
       (st = dalloc(p, &p->d_all, nview)) || (st = dalloc(p, &p->d_idx, nview)) ||
-      (st = dalloc(p, &p->d_H, (size_t)p->nset * ny * g.Hz * Npx)) ||
+      (st = dalloc(p, &p->d_H, (size_t)p->nset * ny * (p->cg.Q + 1) * Npx)) ||
       (st = dalloc(p, &p->d_P, (size_t)p->gmax * p->N)) ||
       (st = dalloc(p, &p->d_part, (size_t)p->gmax * p->nchunk_max * p->nxz)) ||
-      (st = dalloc(p, &p->d_Vhat, (size_t)p->gmax * g.Hz * Npx)) ||
+      (st = dalloc(p, &p->d_Vs, (size_t)p->gmax * p->cg.Q * Npx)) ||
       (st = dalloc(p, &p->d_imgpart, (size_t)p->nsplit_adj * p->N)))
     return bail(st);
 
@@ -624,17 +659,20 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
     const size_t batch = std::max<size_t>(1, std::min(nplanes, ((size_t)256 << 20) / per_plane_G));
     double2 *d_wx = nullptr, *d_wz = nullptr, *d_G = nullptr;
     float* d_psf = nullptr;
+    float* d_Hfull = nullptr;
     auto cleanup = [&]() {
       if (d_wx) cudaFree(d_wx);
       if (d_wz) cudaFree(d_wz);
       if (d_G) cudaFree(d_G);
       if (d_psf) cudaFree(d_psf);
+      if (d_Hfull) cudaFree(d_Hfull);
     };
     cudaError_t e = cudaSuccess;
     e = cudaMalloc((void**)&d_wx, sizeof(double2) * Npx);
     if (e == cudaSuccess) e = cudaMalloc((void**)&d_wz, sizeof(double2) * Npz);
     if (e == cudaSuccess) e = cudaMalloc((void**)&d_G, per_plane_G * batch);
     if (e == cudaSuccess) e = cudaMalloc((void**)&d_psf, sizeof(float) * pp * batch);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&d_Hfull, sizeof(float) * g.Hz * Npx * batch);
     if (e == cudaSuccess) e = cudaMemcpy(d_wx, wx.data(), sizeof(double2) * Npx, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_wz, wz.data(), sizeof(double2) * Npz, cudaMemcpyHostToDevice);
     std::vector<float> hp(pp * batch);
@@ -650,7 +688,11 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
       int blocks = std::min(cdiv((long long)nb * pz * Npx, 256), p->sm_count * 32);
       k_psf_stage1<<<blocks, 256>>>(d_psf, (int)nb, px, pz, Npx, d_wx, d_G);
       blocks = std::min(cdiv((long long)nb * g.Hz * Npx, 256), p->sm_count * 32);
-      k_psf_stage2<<<blocks, 256>>>(d_G, (int)nb, pz, Npx, Npz, g.Hz, d_wz, p->d_H + b0 * g.Hz * Npx);
+      k_psf_stage2<<<blocks, 256>>>(d_G, (int)nb, pz, Npx, Npz, g.Hz, d_wz, d_Hfull);
+      const ConvGeom& cg = p->cg;
+      blocks = std::min(cdiv((long long)nb * (cg.Q + 1) * Npx, 256), p->sm_count * 32);
+      k_psf_permute<<<blocks, 256>>>(d_Hfull, (int)nb, Npx, Npz, g.Hz, p->RX, cg.logCX, p->RZ, cg.logCZ, cg.Q,
+                                     p->d_H + b0 * (cg.Q + 1) * Npx);
       e = cudaGetLastError();
       if (e == cudaSuccess) e = cudaDeviceSynchronize();
     }

@@ -6,20 +6,10 @@
 //                write P[slot][y][z][x] = exp(-dy*(sum_{j<y} mu_j + mu_y/2)) * R(image)
 //                (src/project.jl:103-116).  One CTA per (z slice, view split);
 //                slices staged in shared memory.
-//   k_conv_fwd   persistent; one work item = (view slot, chunk of depth planes).
-//                Per plane: replicate-padded real z-FFT of row pairs, x-FFT of
-//                every kz column with replicate padding, multiply by the
-//                plane's precomputed real PSF spectrum, inverse x-FFT, crop,
-//                inverse z-FFT, crop, accumulate over depth in shared memory
-//                (fft_conv!, src/fft_convolve.jl:33-55, and the depth sum of
-//                src/project.jl:127-130).
+//   k_conv_fwd2  (conv2.cuh) depth-dependent PSF convolution and depth sum.
 //   k_reduce_views  sum of the chunk partials in chunk order (+ fused EM ratio).
 // Adjoint pass (backproject!, src/backproject.jl:277-332):
-//   k_vspec      2-D spectrum of each zero-padded view (shared by all planes).
-//   k_conv_adj   persistent; per plane: spectrum * PSF spectrum, inverse x-FFT,
-//                adjoint of replicate padding along x, inverse z-FFT, adjoint
-//                of replicate padding along z (fft_conv_adj!,
-//                src/fft_convolve.jl:82-130) -> T[slot][y][z][x].
+//   k_vspec2, k_conv_adj2 (conv2.cuh) adjoint PSF convolution -> T[slot][y][z][x].
 //   k_rot_adj    attenuation weighting and the exact transpose of the
 //                bilinear rotation (imrotate_adj! :two, src/rotatez.jl:390-416),
 //                atomic-free: rotated-grid points are scattered in 9 passes by
@@ -30,12 +20,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "fft_warp.cuh"
 
 namespace spect {
-
-constexpr int kConvThreads = 512;
-constexpr int kConvWarps = kConvThreads / 32;
 
 struct Geom {
   int nx, ny, nz;
@@ -128,331 +114,6 @@ __global__ void __launch_bounds__(1024) k_rot_fwd(Geom g, const float* __restric
       float a = expf(__fmul_rn(e, mdy));
       out[(size_t)y * nz * nx] = __fmul_rn(f, a);
       prefix = __fadd_rn(prefix, m);
-    }
-  }
-}
-
-// ------------------------------------------------------------------------
-struct ConvArgs {
-  Geom g;
-  const float* P;       // forward: [nv][ny][nz][nx] rotated+attenuated planes
-  float* T;             // adjoint: [nv][ny][nz][nx] output planes
-  const float* H;       // [nset][ny][Hz][Npx] real PSF spectra (scaled by 1/(Npx*Npz))
-  const int* vidx;      // [nv] plan view index of each slot
-  const int* viewset;   // [nview] spectrum set of each plan view
-  const float2* Vhat;   // adjoint: [nv][Hz][Npx] view spectra
-  float2* VhatOut;      // k_vspec output
-  const float* views;   // k_vspec input [nv][nz][nx]
-  int nv, chunkY, nchunks;
-  float* part;          // forward: [nv][nchunks][nz][nx]
-  float2* gB;           // global fallback for B, per CTA nx*Hz
-  float* gacc;          // global fallback for acc/tbuf, per CTA nz*(nx+2)
-  const float2* tw;     // twiddle table (global)
-  int bsmem, asmem;     // whether B / acc live in shared memory
-};
-
-struct ConvSmem {
-  float2* tw;
-  float2* scratch;  // this warp's line buffer
-  float2* B;        // nx rows x Hz complex (mixed domain: x spatial, kz frequency)
-  float* acc;       // nz x (nx+2) accumulator / output staging
-};
-
-__device__ __forceinline__ ConvSmem conv_smem_setup(const ConvArgs& a, int maxN) {
-  extern __shared__ float4 smem4[];
-  ConvSmem s;
-  const int warp = threadIdx.x >> 5;
-  s.tw = reinterpret_cast<float2*>(smem4);
-  float2* scr = s.tw + SPECT_TW_N;
-  s.scratch = scr + warp * maxN;
-  float2* after = scr + kConvWarps * maxN;
-  size_t Bn = (size_t)a.g.nx * a.g.Hz;
-  if (a.bsmem) {
-    s.B = after;
-    after += Bn;
-  } else {
-    s.B = a.gB + (size_t)blockIdx.x * Bn;
-  }
-  size_t An = (size_t)a.g.nz * (a.g.nx + 2);
-  if (a.asmem) s.acc = reinterpret_cast<float*>(after);
-  else s.acc = a.gacc + (size_t)blockIdx.x * An;
-  for (int k = threadIdx.x; k < SPECT_TW_N; k += blockDim.x) s.tw[k] = a.tw[k];
-  __syncthreads();
-  return s;
-}
-
-// z-FFT of row pairs (x0, x0+1) read from real rows of B (row stride 2*Hz
-// floats); ZEROPAD selects zero padding (adjoint) instead of replication.
-template <bool ZEROPAD>
-__device__ __forceinline__ void stage_zfft_rows(const Geom& g, ConvSmem& s, int warp, int lane) {
-  const int Hz = g.Hz, Npz = g.Npz, nz = g.nz, nx = g.nx;
-  float* Bf = reinterpret_cast<float*>(s.B);
-  for (int rp = warp; rp < (nx >> 1); rp += kConvWarps) {
-    const int x0 = 2 * rp;
-    const float* r0 = Bf + (size_t)x0 * 2 * Hz;
-    const float* r1 = r0 + 2 * Hz;
-    for (int zz = lane; zz < Npz; zz += 32) {
-      int zc = zz - g.padleft;
-      float2 v;
-      if (ZEROPAD) {
-        bool in = (unsigned)zc < (unsigned)nz;
-        v = in ? make_float2(r0[zc], r1[zc]) : make_float2(0.f, 0.f);
-      } else {
-        zc = min(max(zc, 0), nz - 1);
-        v = make_float2(r0[zc], r1[zc]);
-      }
-      s.scratch[zz] = v;
-    }
-    __syncwarp();
-    warp_fft<false>(s.scratch, Npz, g.logNpz, s.tw, lane);
-    // unpack the two real rows: A[k] = (Z[k] + conj Z[-k]) / 2, B[k] = (Z[k] - conj Z[-k]) / 2i
-    for (int k = lane; k < Hz; k += 32) {
-      float2 zk = s.scratch[k], zn = s.scratch[(Npz - k) & (Npz - 1)];
-      s.B[(size_t)x0 * Hz + k] = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
-      s.B[(size_t)(x0 + 1) * Hz + k] = make_float2(0.5f * (zk.y + zn.y), 0.5f * (zn.x - zk.x));
-    }
-    __syncwarp();
-  }
-}
-
-// transposed load of a real nz x nx plane (x fastest in memory) into the real
-// rows of B: Bf[x][z].
-__device__ __forceinline__ void stage_load_plane(const Geom& g, ConvSmem& s, const float* __restrict__ src) {
-  float* Bf = reinterpret_cast<float*>(s.B);
-  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.Hz;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    int z = k / nx, x = k - z * nx;
-    Bf[(size_t)x * rs + z] = __ldg(src + k);
-  }
-}
-
-// build the Hermitian-extended spectrum of the row pair (x0, x0+1) in scratch
-__device__ __forceinline__ void hermitian_pair(const Geom& g, ConvSmem& s, int x0, int lane) {
-  const int Hz = g.Hz, Npz = g.Npz;
-  const float2* b0 = s.B + (size_t)x0 * Hz;
-  const float2* b1 = b0 + Hz;
-  for (int k = lane; k < Npz; k += 32) {
-    float2 a, b;
-    if (k < Hz) {
-      a = b0[k];
-      b = b1[k];
-      if (k == 0 || k == Hz - 1) {  // DC / Nyquist bins of a real row are real
-        a.y = 0.f;
-        b.y = 0.f;
-      }
-    } else {
-      a = b0[Npz - k];
-      b = b1[Npz - k];
-      a.y = -a.y;
-      b.y = -b.y;
-    }
-    s.scratch[k] = make_float2(a.x - b.y, a.y + b.x);  // a + i b
-  }
-  __syncwarp();
-}
-
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// ------------------------------------------------------------------------
-// k_conv_fwd: persistent over items (slot, chunk).
-__global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd(ConvArgs a) {
-  const Geom& g = a.g;
-  const int maxN = max(g.Npx, g.Npz);
-  ConvSmem s = conv_smem_setup(a, maxN);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, Hz = g.Hz, Npx = g.Npx;
-  const int AS = nx + 2;
-  const int nitems = a.nv * a.nchunks;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int slot = item / a.nchunks, c = item - slot * a.nchunks;
-    const int y0 = c * a.chunkY, y1 = min(ny, y0 + a.chunkY);
-    const float* Pv = a.P + (size_t)slot * ny * nz * nx;
-    const float* Hv = a.H + (size_t)a.viewset[a.vidx[slot]] * ny * Hz * Npx;
-    for (int y = y0; y < y1; ++y) {
-      __syncthreads();  // B and scratch free
-      stage_load_plane(g, s, Pv + (size_t)y * nz * nx);
-      __syncthreads();
-      stage_zfft_rows<false>(g, s, warp, lane);
-      __syncthreads();
-      // x-FFT per kz column, multiply by the PSF spectrum, inverse, crop
-      const float* Hy = Hv + (size_t)y * Hz * Npx;
-      for (int kz = warp; kz < Hz; kz += kConvWarps) {
-        for (int xx = lane; xx < Npx; xx += 32) {
-          int xc = min(max(xx - g.padup, 0), nx - 1);
-          s.scratch[xx] = s.B[(size_t)xc * Hz + kz];
-        }
-        __syncwarp();
-        warp_fft<false>(s.scratch, Npx, g.logNpx, s.tw, lane);
-        const float* h = Hy + (size_t)kz * Npx;
-        for (int kx = lane; kx < Npx; kx += 32) {
-          float hv = __ldg(h + kx);
-          float2 v = s.scratch[kx];
-          s.scratch[kx] = make_float2(v.x * hv, v.y * hv);
-        }
-        __syncwarp();
-        warp_fft<true>(s.scratch, Npx, g.logNpx, s.tw, lane);
-        for (int x = lane; x < nx; x += 32) s.B[(size_t)x * Hz + kz] = s.scratch[g.padup + x];
-        __syncwarp();
-      }
-      __syncthreads();
-      // inverse z-FFT of row pairs, crop, accumulate over depth
-      const bool first = (y == y0);
-      for (int rp = warp; rp < (nx >> 1); rp += kConvWarps) {
-        const int x0 = 2 * rp;
-        hermitian_pair(g, s, x0, lane);
-        warp_fft<true>(s.scratch, g.Npz, g.logNpz, s.tw, lane);
-        for (int z = lane; z < nz; z += 32) {
-          float2 r = s.scratch[g.padleft + z];
-          float2* o = reinterpret_cast<float2*>(s.acc + (size_t)z * AS + x0);
-          if (first) {
-            *o = r;
-          } else {
-            float2 p = *o;
-            *o = make_float2(p.x + r.x, p.y + r.y);
-          }
-        }
-        __syncwarp();
-      }
-    }
-    __syncthreads();
-    float* dst = a.part + ((size_t)slot * a.nchunks + c) * nz * nx;
-    for (int k = threadIdx.x; k < nz * nx; k += blockDim.x) {
-      int z = k / nx, x = k - z * nx;
-      dst[k] = s.acc[(size_t)z * AS + x];
-    }
-  }
-}
-
-// ------------------------------------------------------------------------
-// k_vspec: spectrum of each zero-padded view, Vhat[slot][kz][kx].
-__global__ void __launch_bounds__(kConvThreads, 1) k_vspec(ConvArgs a) {
-  const Geom& g = a.g;
-  const int maxN = max(g.Npx, g.Npz);
-  ConvSmem s = conv_smem_setup(a, maxN);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nx = g.nx, nz = g.nz, Hz = g.Hz, Npx = g.Npx;
-  for (int slot = blockIdx.x; slot < a.nv; slot += gridDim.x) {
-    __syncthreads();
-    stage_load_plane(g, s, a.views + (size_t)slot * nz * nx);
-    __syncthreads();
-    stage_zfft_rows<true>(g, s, warp, lane);
-    __syncthreads();
-    for (int kz = warp; kz < Hz; kz += kConvWarps) {
-      for (int xx = lane; xx < Npx; xx += 32) {
-        int xc = xx - g.padup;
-        s.scratch[xx] = ((unsigned)xc < (unsigned)nx) ? s.B[(size_t)xc * Hz + kz] : make_float2(0.f, 0.f);
-      }
-      __syncwarp();
-      warp_fft<false>(s.scratch, Npx, g.logNpx, s.tw, lane);
-      float2* out = a.VhatOut + ((size_t)slot * Hz + kz) * Npx;
-      for (int kx = lane; kx < Npx; kx += 32) out[kx] = s.scratch[kx];
-      __syncwarp();
-    }
-  }
-}
-
-// ------------------------------------------------------------------------
-// k_conv_adj: persistent over items (slot, chunk); T[slot][y][z][x].
-__global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj(ConvArgs a) {
-  const Geom& g = a.g;
-  const int maxN = max(g.Npx, g.Npz);
-  ConvSmem s = conv_smem_setup(a, maxN);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, Hz = g.Hz, Npx = g.Npx, Npz = g.Npz;
-  const int AS = nx + 2;
-  const int nitems = a.nv * a.nchunks;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int slot = item / a.nchunks, c = item - slot * a.nchunks;
-    const int y0 = c * a.chunkY, y1 = min(ny, y0 + a.chunkY);
-    const float* Hv = a.H + (size_t)a.viewset[a.vidx[slot]] * ny * Hz * Npx;
-    const float2* Vs = a.Vhat + (size_t)slot * Hz * Npx;
-    for (int y = y0; y < y1; ++y) {
-      __syncthreads();
-      const float* Hy = Hv + (size_t)y * Hz * Npx;
-      for (int kz = warp; kz < Hz; kz += kConvWarps) {
-        const float* h = Hy + (size_t)kz * Npx;
-        const float2* vk = Vs + (size_t)kz * Npx;
-        for (int kx = lane; kx < Npx; kx += 32) {
-          float hv = __ldg(h + kx);
-          float2 v = vk[kx];
-          s.scratch[kx] = make_float2(v.x * hv, v.y * hv);
-        }
-        __syncwarp();
-        warp_fft<true>(s.scratch, Npx, g.logNpx, s.tw, lane);
-        // adjoint of replicate padding along x: fold the pad rows into the edges
-        float lr = 0.f, li = 0.f, hr = 0.f, hi = 0.f;
-        for (int xx = lane; xx < g.padup; xx += 32) {
-          float2 v = s.scratch[xx];
-          lr += v.x;
-          li += v.y;
-        }
-        for (int xx = g.padup + nx + lane; xx < Npx; xx += 32) {
-          float2 v = s.scratch[xx];
-          hr += v.x;
-          hi += v.y;
-        }
-        lr = warp_sum(lr);
-        li = warp_sum(li);
-        hr = warp_sum(hr);
-        hi = warp_sum(hi);
-        for (int x = lane; x < nx; x += 32) {
-          float2 v = s.scratch[g.padup + x];
-          if (x == 0) {
-            v.x += lr;
-            v.y += li;
-          }
-          if (x == nx - 1) {
-            v.x += hr;
-            v.y += hi;
-          }
-          s.B[(size_t)x * Hz + kz] = v;
-        }
-        __syncwarp();
-      }
-      __syncthreads();
-      for (int rp = warp; rp < (nx >> 1); rp += kConvWarps) {
-        const int x0 = 2 * rp;
-        hermitian_pair(g, s, x0, lane);
-        warp_fft<true>(s.scratch, Npz, g.logNpz, s.tw, lane);
-        float lr = 0.f, li = 0.f, hr = 0.f, hi = 0.f;
-        for (int zz = lane; zz < g.padleft; zz += 32) {
-          float2 v = s.scratch[zz];
-          lr += v.x;
-          li += v.y;
-        }
-        for (int zz = g.padleft + nz + lane; zz < Npz; zz += 32) {
-          float2 v = s.scratch[zz];
-          hr += v.x;
-          hi += v.y;
-        }
-        lr = warp_sum(lr);
-        li = warp_sum(li);
-        hr = warp_sum(hr);
-        hi = warp_sum(hi);
-        for (int z = lane; z < nz; z += 32) {
-          float2 v = s.scratch[g.padleft + z];
-          if (z == 0) {
-            v.x += lr;
-            v.y += li;
-          }
-          if (z == nz - 1) {
-            v.x += hr;
-            v.y += hi;
-          }
-          *reinterpret_cast<float2*>(s.acc + (size_t)z * AS + x0) = v;
-        }
-        __syncwarp();
-      }
-      __syncthreads();
-      float* dst = a.T + ((size_t)slot * ny + y) * nz * nx;
-      for (int k = threadIdx.x; k < nz * nx; k += blockDim.x) {
-        int z = k / nx, x = k - z * nx;
-        dst[k] = s.acc[(size_t)z * AS + x];
-      }
     }
   }
 }
@@ -635,6 +296,34 @@ __global__ void k_psf_stage2(const double2* __restrict__ G, int nplanes, int pz,
       re += gv.x * w.x - gv.y * w.y;
     }
     H[k] = (float)(re * scale);
+  }
+}
+
+// Hs[pl][c][k1x*CX + lx] in the scrambled orders of the conv kernels
+// (conv2.cuh) from H[pl][kz][kx] (kz < Npz/2+1).
+__global__ void k_psf_permute(const float* __restrict__ H, int nplanes, int Npx, int Npz, int Hz, int RX, int logCX,
+                              int RZ, int logCZ, int Q, float* __restrict__ Hs) {
+  const size_t n = (size_t)nplanes * (Q + 1) * Npx;
+  const int CX = 1 << logCX, CZ = 1 << logCZ, half = CZ >> 1;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const int pos = (int)(k % Npx);
+    const size_t r = k / Npx;
+    const int c = (int)(r % (Q + 1));
+    const size_t pl = r / (Q + 1);
+    const int k1 = pos / CX, l = pos - k1 * CX;
+    const int kx = k1 + RX * (logCX ? (int)(__brev(l) >> (32 - logCX)) : 0);
+    const float* Hp = H + pl * Hz * Npx;
+    float v;
+    if (c == 0 || c == Q) {
+      float h0 = Hp[kx], hn = (Npz >= 2) ? Hp[(size_t)(Npz / 2) * Npx + kx] : 0.f;
+      if (Npz >= 2) v = (c == 0) ? 0.5f * (h0 + hn) : 0.5f * (h0 - hn);
+      else v = (c == 0) ? h0 : 0.f;
+    } else {
+      const int k1z = c / half, lz = 2 * (c - k1z * half);
+      const int kz = k1z + RZ * (logCZ ? (int)(__brev(lz) >> (32 - logCZ)) : 0);
+      v = Hp[(size_t)kz * Npx + kx];
+    }
+    Hs[k] = v;
   }
 }
 
