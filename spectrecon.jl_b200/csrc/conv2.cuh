@@ -73,13 +73,14 @@ __device__ __forceinline__ Lanes lanes_of(int lane, int logC) {
   return L;
 }
 
-__device__ __forceinline__ float2* conv_setup(const Conv2Args& a, float2** twp) {
+// shared memory: [FFT tables (fft_tables_bytes(RX, RZ))][B when bsmem]
+template <int RX, int RZ>
+__device__ __forceinline__ float2* conv_setup(const Conv2Args& a, FftTables* T) {
   extern __shared__ float4 smem4[];
-  float2* tw = reinterpret_cast<float2*>(smem4);
-  for (int k = threadIdx.x; k < SPECT_TW_N; k += blockDim.x) tw[k] = a.tw[k];
-  *twp = tw;
+  float2* base = reinterpret_cast<float2*>(smem4);
+  *T = build_fft_tables(base, a.tw, RX, a.g.logNpx, RZ, a.g.logNpz);
   __syncthreads();
-  if (a.bsmem) return tw + SPECT_TW_N;
+  if (a.bsmem) return base + fft_tables_bytes(RX, RZ) / 8;
   return a.gB + (size_t)blockIdx.x * a.g.nx * a.g.QS;
 }
 
@@ -194,7 +195,7 @@ struct LaneTables {
 // z transform of row pairs (x0, x0+1), in place in B: real rows -> stored
 // columns.  ZEROPAD: zero padding (adjoint) instead of replication.
 template <int RZ, bool ZEROPAD>
-__device__ __forceinline__ void zfft_rows_fwd(const ConvGeom& g, float2* B, const float2* __restrict__ tw, int warp,
+__device__ __forceinline__ void zfft_rows_fwd(const ConvGeom& g, float2* B, const FftTables& TT, int warp,
                                               int lane, const int (&zrd)[RZ]) {
   const Lanes L = lanes_of(lane, g.logCZ);
   const int CZ = g.CZ, GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
@@ -215,7 +216,7 @@ __device__ __forceinline__ void zfft_rows_fwd(const ConvGeom& g, float2* B, cons
       else v[r] = make_float2(r0[zc], r1[zc]);
     }
     __syncwarp();
-    fft_fwd<RZ>(v, L.l, g.logCZ, g.logNpz, tw);
+    fft_fwd<RZ>(v, L.l, g.logCZ, TT, TT.rz + L.l);
     // partners: register k1 <-> RZ-k1 in lane l ^ (CZ-1); register 0 via brev
     float2 p[RZ];
     p[0] = shfl2(v[0], L.gbase + brev_rt((CZ - brev_rt(L.l, g.logCZ)) & (CZ - 1), g.logCZ));
@@ -275,8 +276,11 @@ __device__ __forceinline__ void gather_zspec(const float2* b0, const float2* b1,
 }
 
 template <int R>
-__device__ __forceinline__ float2 group_sum(float2 s, int logC) {
-  for (int q = 0; q < logC; ++q) s = cadd(s, shfl_xor2(s, 1 << q));
+__device__ __forceinline__ float2 group_sum(float2 s, int logC_rt) {
+  const int logC = (R > 1) ? 5 : logC_rt;
+#pragma unroll
+  for (int q = 0; q < 5; ++q)
+    if (q < logC) s = cadd(s, shfl_xor2(s, 1 << q));
   return s;
 }
 
@@ -286,7 +290,7 @@ __device__ __forceinline__ float2 group_sum(float2 s, int logC) {
 // be non-zero (zero-padded input, PSF half width hz, no wrap-around since the
 // pads are >= hz), so only those are summed; the rest hold FFT round-off.
 template <int RZ, bool FOLD>
-__device__ __forceinline__ void zfft_rows_inv(const ConvGeom& g, float2* B, const float2* __restrict__ tw, int warp,
+__device__ __forceinline__ void zfft_rows_inv(const ConvGeom& g, float2* B, const FftTables& TT, int warp,
                                               int lane, const int (&zg)[RZ]) {
   const Lanes L = lanes_of(lane, g.logCZ);
   const int CZ = g.CZ, GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
@@ -300,7 +304,7 @@ __device__ __forceinline__ void zfft_rows_inv(const ConvGeom& g, float2* B, cons
     float2 v[RZ];
     gather_zspec<RZ>(B + x0 * QS, B + (x0 + 1) * QS, zg, v);
     __syncwarp();
-    fft_inv<RZ>(v, L.l, g.logCZ, g.logNpz, tw);
+    fft_inv<RZ>(v, L.l, g.logCZ, TT, TT.rz + L.l);
     float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
     if (FOLD) {
 #pragma unroll
@@ -338,7 +342,7 @@ __device__ __forceinline__ void zfft_rows_inv(const ConvGeom& g, float2* B, cons
 template <int RX>
 __device__ __forceinline__ void apply_psf(float2 (&v)[RX], const float* __restrict__ h, const float* __restrict__ hb,
                                           const Lanes& L, int logCX, bool packed_warp, bool col0) {
-  const int CX = 1 << logCX;
+  const int CX = (RX > 1) ? 32 : (1 << logCX);
   if (packed_warp) {
     // Y' = alpha Y + beta conj(Y(-k)); registers k1 and RX-k1 are partners
     const int src0 = L.gbase + brev_rt((CX - brev_rt(L.l, logCX)) & (CX - 1), logCX);
@@ -370,11 +374,11 @@ __device__ __forceinline__ void apply_psf(float2 (&v)[RX], const float* __restri
 template <int RX, int RZ, bool REGACC>
 __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
   const ConvGeom& g = a.g;
-  float2* tw;
-  float2* B = conv_setup(a, &tw);
+  FftTables TT;
+  float2* B = conv_setup<RX, RZ>(a, &TT);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Lanes L = lanes_of(lane, g.logCX);
-  const int CX = g.CX, GX = 32 >> g.logCX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
+  const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
   const int JC = (Q + units - 1) / units;
   constexpr int JM = RZ > 1 ? RZ : 1;
   const int nitems = a.nv * a.nchunks;
@@ -392,7 +396,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
       __syncthreads();
       load_plane(g, W, B, Pv + (size_t)y * g.nz * g.nx);
       __syncthreads();
-      zfft_rows_fwd<RZ, false>(g, B, tw, warp, lane, T.zrd);
+      zfft_rows_fwd<RZ, false>(g, B, TT, warp, lane, T.zrd);
       __syncthreads();
       const float* Hy = Hv + (size_t)y * (Q + 1) * Npx;
 #pragma unroll
@@ -404,7 +408,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
           float2 v[RX];
 #pragma unroll
           for (int r = 0; r < RX; ++r) v[r] = B[T.xrd[r] + cc];
-          fft_fwd<RX>(v, L.l, g.logCX, g.logNpx, tw);
+          fft_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
           apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX,
                         j == 0 && warp == 0, cc == 0);
           if (active) {
@@ -438,7 +442,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
 #pragma unroll
           for (int k1 = 0; k1 < RX; ++k1) v[k1] = ga[k1 * CX];
         }
-        fft_inv<RX>(v, L.l, g.logCX, g.logNpx, tw);
+        fft_inv<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
         if (active) {
 #pragma unroll
           for (int r = 0; r < RX; ++r)
@@ -447,7 +451,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
       }
     }
     __syncthreads();
-    zfft_rows_inv<RZ, false>(g, B, tw, warp, lane, TW.zg);
+    zfft_rows_inv<RZ, false>(g, B, TT, warp, lane, TW.zg);
     __syncthreads();
     store_plane(g, W, B, a.part + ((size_t)slot * a.nchunks + ch) * g.nz * g.nx);
   }
@@ -458,11 +462,11 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
 template <int RX, int RZ>
 __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
   const ConvGeom& g = a.g;
-  float2* tw;
-  float2* B = conv_setup(a, &tw);
+  FftTables TT;
+  float2* B = conv_setup<RX, RZ>(a, &TT);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Lanes L = lanes_of(lane, g.logCX);
-  const int CX = g.CX, GX = 32 >> g.logCX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
+  const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
   const int iters = (Q + units - 1) / units;
   const PlaneWalk W(g.nx);
   LaneTables<RX, RZ> T;
@@ -471,7 +475,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
     __syncthreads();
     load_plane(g, W, B, a.views + (size_t)slot * g.nz * g.nx);
     __syncthreads();
-    zfft_rows_fwd<RZ, true>(g, B, tw, warp, lane, T.zrd);
+    zfft_rows_fwd<RZ, true>(g, B, TT, warp, lane, T.zrd);
     __syncthreads();
     for (int it = 0; it < iters; ++it) {
       const int c = it * units + warp * GX + L.g;
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
       float2 v[RX];
 #pragma unroll
       for (int r = 0; r < RX; ++r) v[r] = (T.xrd[r] >= 0) ? B[T.xrd[r] + cc] : make_float2(0.f, 0.f);
-      fft_fwd<RX>(v, L.l, g.logCX, g.logNpx, tw);
+      fft_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
       if (c < Q) {
         float2* o = a.VsOut + ((size_t)slot * Q + c) * Npx + L.l;
 #pragma unroll
@@ -494,11 +498,11 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
 template <int RX, int RZ, bool REGACC>
 __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
   const ConvGeom& g = a.g;
-  float2* tw;
-  float2* B = conv_setup(a, &tw);
+  FftTables TT;
+  float2* B = conv_setup<RX, RZ>(a, &TT);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Lanes L = lanes_of(lane, g.logCX);
-  const int CX = g.CX, GX = 32 >> g.logCX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
+  const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
   const int JC = (Q + units - 1) / units;
   constexpr int JM = RZ > 1 ? RZ : 1;
   const int nitems = a.nv * a.nchunks;
@@ -536,7 +540,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
             v[k1] = REGACC ? vs[REGACC ? j : 0][k1] : Vsl[(size_t)cc * Npx + L.l + k1 * CX];
           apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX,
                         j == 0 && warp == 0, cc == 0);
-          fft_inv<RX>(v, L.l, g.logCX, g.logNpx, tw);
+          fft_inv<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
           // adjoint of the replicate padding along x
           float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
 #pragma unroll
@@ -562,7 +566,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
         }
       }
       __syncthreads();
-      zfft_rows_inv<RZ, true>(g, B, tw, warp, lane, T.zg);
+      zfft_rows_inv<RZ, true>(g, B, TT, warp, lane, T.zg);
       __syncthreads();
       store_plane(g, W, B, a.T + ((size_t)slot * g.ny + y) * g.nz * g.nx);
     }

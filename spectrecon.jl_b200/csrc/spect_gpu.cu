@@ -24,6 +24,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -154,6 +155,7 @@ struct spect_plan_s {
   size_t N = 0, nxz = 0;
   // device
   float* d_mumap = nullptr;
+  float* d_att = nullptr;  // [nview][ny][nz][nx] attenuation cache (optional)
   float* d_H = nullptr;
   float4* d_rot = nullptr;
   int* d_viewset = nullptr;
@@ -185,6 +187,7 @@ struct spect_plan_s {
   size_t conv_smem = 0;
   int rotf_vpb = 1, rotf_smem_ok = 1;
   size_t rotf_smem = 0;
+  int att_smem_ok = 1;
   int rota_smem_ok = 1, nsplit_adj = 1;
   size_t rota_smem = 0;
   size_t bytes = 0;
@@ -209,7 +212,7 @@ int dalloc(spect_plan_s* p, T** ptr, size_t count) {
 }
 
 void free_plan(spect_plan_s* p) {
-  void* ptrs[] = {p->d_mumap, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
+  void* ptrs[] = {p->d_mumap, p->d_att, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag,
                   p->d_io_img, p->d_io_views};
@@ -273,7 +276,7 @@ int configure(spect_plan_s* p) {
   cg.logCZ = ilog2(cg.CZ);
   p->RX = g.Npx / cg.CX;
   p->RZ = g.Npz / cg.CZ;
-  size_t base = sizeof(float2) * SPECT_TW_N;
+  size_t base = (size_t)fft_tables_bytes(p->RX, p->RZ);
   size_t Bb = sizeof(float2) * (size_t)g.nx * cg.QS;
   p->conv_bsmem = (base + Bb <= p->max_smem) ? 1 : 0;
   p->conv_smem = base + (p->conv_bsmem ? Bb : 0);
@@ -293,18 +296,26 @@ int configure(spect_plan_s* p) {
   // ---- forward rotation
   p->rotf_vpb = std::max(1, std::min(8, 512 / g.nx));
   size_t slice = (size_t)g.nx * g.ny;
-  p->rotf_smem = 2 * slice * sizeof(float);
+  // staged slices: image (+ mu-map when the attenuation is not cached)
+  p->rotf_smem = (p->d_att ? 1 : 2) * slice * sizeof(float);
   p->rotf_smem_ok = p->rotf_smem <= p->max_smem;
-  if (p->rotf_smem_ok)
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)p->rotf_smem));
+  if (p->rotf_smem_ok) {
+    const void* kf = p->d_att ? (const void*)k_rot_fwd<true, true> : (const void*)k_rot_fwd<true, false>;
+    CUDA_TRY(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->rotf_smem));
+  }
+  p->att_smem_ok = slice * sizeof(float) <= p->max_smem;
+  if (p->att_smem_ok)
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_atten_build<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(slice * sizeof(float))));
   // ---- adjoint rotation
   int nseg = std::max(1, kRotAdjThreads / g.nx);
   p->rota_smem = (2 * slice + (size_t)nseg * g.nx) * sizeof(float);
   p->rota_smem_ok = p->rota_smem <= p->max_smem;
   p->nsplit_adj = std::max(1, std::min(8, cdiv(2 * p->sm_count, g.nz)));
   if (p->rota_smem_ok) {
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)p->rota_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)p->rota_smem));
   } else {
     size_t per = 2 * slice + (size_t)nseg * g.nx;
@@ -359,10 +370,17 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
     int vpb = p->rotf_vpb;
     int nsplit = std::max(1, std::min(cdiv(2 * p->sm_count, g.nz), cdiv(nv, vpb)));
     dim3 grid(g.nz, nsplit);
+    const int thr = g.nx * vpb;
+    const float* att = p->d_att;
     LAUNCH(p, K_ROT_FWD, st, "k_rot_fwd",
-           if (p->rotf_smem_ok) k_rot_fwd<true><<<grid, g.nx * vpb, p->rotf_smem, st>>>(g, image, p->d_mumap,
-                                                                                         p->d_rot, vi, nv, p->d_P);
-           else k_rot_fwd<false><<<grid, g.nx * vpb, 0, st>>>(g, image, p->d_mumap, p->d_rot, vi, nv, p->d_P));
+           if (p->rotf_smem_ok && att) k_rot_fwd<true, true><<<grid, thr, p->rotf_smem, st>>>(
+               g, image, p->d_mumap, att, p->d_rot, vi, nv, p->d_P);
+           else if (p->rotf_smem_ok) k_rot_fwd<true, false><<<grid, thr, p->rotf_smem, st>>>(
+               g, image, p->d_mumap, att, p->d_rot, vi, nv, p->d_P);
+           else if (att) k_rot_fwd<false, true><<<grid, thr, 0, st>>>(g, image, p->d_mumap, att, p->d_rot, vi, nv,
+                                                                      p->d_P);
+           else k_rot_fwd<false, false><<<grid, thr, 0, st>>>(g, image, p->d_mumap, att, p->d_rot, vi, nv,
+                                                              p->d_P));
     // FFT convolution + depth sum -> part
     Conv2Args a = conv_args(p);
     int cy, nc;
@@ -412,9 +430,13 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     a.nchunks = nc;
     LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj", conv_launch(p, 1, std::min(p->conv_grid, nv * nc), st, a));
     dim3 grid(g.nz, nsplit);
+    const size_t rsm = p->rota_smem_ok ? p->rota_smem : 0;
     LAUNCH(p, K_ROT_ADJ, st, "k_rot_adj",
-           k_rot_adj<<<grid, kRotAdjThreads, p->rota_smem_ok ? p->rota_smem : 0, st>>>(
-               g, p->d_P, p->d_mumap, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
+           if (p->d_att) k_rot_adj<true><<<grid, kRotAdjThreads, rsm, st>>>(
+               g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
+               p->d_gscr_adj);
+           else k_rot_adj<false><<<grid, kRotAdjThreads, rsm, st>>>(
+               g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
                p->d_gscr_adj));
   }
   int rb = (int)std::min<size_t>((p->N + 255) / 256, (size_t)p->sm_count * 16);
@@ -585,6 +607,21 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
     free_plan(p);
     return st;
   };
+  // attenuation cache (nview * N floats): on when it fits a quarter of the
+  // free device memory (and 32 GiB); SPECT_ATTEN_CACHE=0 turns it off
+  {
+    const char* env = std::getenv("SPECT_ATTEN_CACHE");
+    size_t need = sizeof(float) * p->N * (size_t)nview, fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      fr = 0;
+    }
+    bool want = !(env && env[0] == '0') && need <= std::min(fr / 4, (size_t)32 << 30);
+    if (want && dalloc(p, &p->d_att, p->N * (size_t)nview) != SPECT_OK) {
+      p->d_att = nullptr;
+      g_err.clear();
+    }
+  }
   int st = configure(p);
   if (st != SPECT_OK) return bail(st);
 
@@ -648,6 +685,21 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
       (st = up(p->d_tw, tw.data(), sizeof(float2) * SPECT_TW_N)) ||
       (st = up(p->d_all, all.data(), sizeof(int) * nview)))
     return bail(st);
+
+  if (p->d_att) {
+    dim3 grid(nz, std::max(1, std::min(cdiv(2 * p->sm_count, nz), cdiv(nview, p->rotf_vpb))));
+    const int thr = nx * p->rotf_vpb;
+    if (p->att_smem_ok)
+      k_atten_build<true><<<grid, thr, sizeof(float) * (size_t)nx * ny>>>(g, p->d_mumap, p->d_rot, nview, p->d_att);
+    else
+      k_atten_build<false><<<grid, thr>>>(g, p->d_mumap, p->d_rot, nview, p->d_att);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+      fail(SPECT_ERR_CUDA, std::string("attenuation cache: ") + cudaGetErrorString(e));
+      return bail(SPECT_ERR_CUDA);
+    }
+  }
 
   // PSF spectra, in batches of planes (double precision on the device)
   {

@@ -65,12 +65,55 @@ __device__ __forceinline__ float bilinear(const float* __restrict__ s, int n, co
 }
 
 // ------------------------------------------------------------------------
-// k_rot_fwd: grid (nz, nsplit), block nx * vpb threads.
-// P[slot][y][z][x] for slots [split range).  SMEM: stage the two slices.
+// Attenuation factors of one view on the rotated grid, by depth scan along y
+// (src/project.jl:103-113): a(x,y,z) = exp(-dy * (sum_{j<y} mu_j + mu_y/2)),
+// mu = R_theta(mumap) (imrotate! :two, with the theta == 0 copy).
+// k_atten_build: grid (nz, nsplit), block nx * vpb; writes att[v][y][z][x]
+// for every plan view (the per-plan attenuation cache).
 template <bool SMEM>
+__global__ void __launch_bounds__(1024) k_atten_build(Geom g, const float* __restrict__ mumap,
+                                                      const float4* __restrict__ rot, int nview,
+                                                      float* __restrict__ att) {
+  extern __shared__ float4 smem4[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz, z = blockIdx.x;
+  const size_t slice = (size_t)nx * ny;
+  const float* sm = mumap + (size_t)z * slice;
+  if (SMEM) {
+    float* ss = reinterpret_cast<float*>(smem4);
+    for (int k = threadIdx.x; k < (int)slice; k += blockDim.x) ss[k] = __ldg(sm + k);
+    __syncthreads();
+    sm = ss;
+  }
+  const int per = (nview + gridDim.y - 1) / gridDim.y;
+  const int v0 = blockIdx.y * per, v1 = min(nview, v0 + per);
+  const int vpb = blockDim.x / nx, sub = threadIdx.x / nx, x = threadIdx.x - sub * nx;
+  if (sub >= vpb) return;
+  const float mdy = -g.dy;
+  for (int v = v0 + sub; v < v1; v += vpb) {
+    const float4 r = rot[v];
+    RotPos R{r.x, r.y, g.c0};
+    const bool ident = r.z != 0.f;
+    float prefix = 0.f;
+    float* out = att + ((size_t)v * ny * nz + z) * nx + x;
+    for (int y = 0; y < ny; ++y) {
+      float m = ident ? sm[x + y * nx] : bilinear(sm, nx, R, x, y);
+      float e = __fadd_rn(prefix, __fmul_rn(0.5f, m));
+      out[(size_t)y * nz * nx] = expf(__fmul_rn(e, mdy));
+      prefix = __fadd_rn(prefix, m);
+    }
+  }
+}
+
+// k_rot_fwd: grid (nz, nsplit), block nx * vpb threads.
+// P[slot][y][z][x] = a(x,y,z) * R_theta(image)(x,y,z) for the launch's slots.
+// CACHED: a read from the attenuation cache att[view][y][z][x]; otherwise
+// the rotated mu-map is scanned here (both slices staged in shared memory
+// when SMEM).
+template <bool SMEM, bool CACHED>
 __global__ void __launch_bounds__(1024) k_rot_fwd(Geom g, const float* __restrict__ image,
-                                                  const float* __restrict__ mumap, const float4* __restrict__ rot,
-                                                  const int* __restrict__ vidx, int nv, float* __restrict__ P) {
+                                                  const float* __restrict__ mumap, const float* __restrict__ att,
+                                                  const float4* __restrict__ rot, const int* __restrict__ vidx, int nv,
+                                                  float* __restrict__ P) {
   extern __shared__ float4 smem4[];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int z = blockIdx.x;
@@ -82,7 +125,7 @@ __global__ void __launch_bounds__(1024) k_rot_fwd(Geom g, const float* __restric
     float* sm = si + slice;
     for (int k = threadIdx.x; k < (int)slice; k += blockDim.x) {
       si[k] = __ldg(img + k);
-      sm[k] = __ldg(mu + k);
+      if (!CACHED) sm[k] = __ldg(mu + k);
     }
     __syncthreads();
     img = si;
@@ -95,25 +138,27 @@ __global__ void __launch_bounds__(1024) k_rot_fwd(Geom g, const float* __restric
   if (sub >= vpb) return;
   const float mdy = -g.dy;
   for (int s = s0 + sub; s < s1; s += vpb) {
-    const float4 r = rot[vidx[s]];
+    const int v = vidx[s];
+    const float4 r = rot[v];
     RotPos R{r.x, r.y, g.c0};
     const bool ident = r.z != 0.f;
     float prefix = 0.f;
     float* out = P + ((size_t)s * ny * nz + z) * nx + x;
+    const float* av = att + ((size_t)v * ny * nz + z) * nx + x;
+#pragma unroll 8
     for (int y = 0; y < ny; ++y) {
-      float f, m;
-      if (ident) {
-        f = img[x + y * nx];
-        m = mu[x + y * nx];
+      const float f = ident ? img[x + y * nx] : bilinear(img, nx, R, x, y);
+      float a;
+      if (CACHED) {
+        a = __ldg(av + (size_t)y * nz * nx);
       } else {
-        f = bilinear(img, nx, R, x, y);
-        m = bilinear(mu, nx, R, x, y);
+        const float m = ident ? mu[x + y * nx] : bilinear(mu, nx, R, x, y);
+        // exp(-dy * (sum_{j<y} mu_j + mu_y/2))  (src/project.jl:103-113)
+        const float e = __fadd_rn(prefix, __fmul_rn(0.5f, m));
+        a = expf(__fmul_rn(e, mdy));
+        prefix = __fadd_rn(prefix, m);
       }
-      // exp(-dy * (sum_{j<y} mu_j + mu_y/2))  (src/project.jl:103-113)
-      float e = __fadd_rn(prefix, __fmul_rn(0.5f, m));
-      float a = expf(__fmul_rn(e, mdy));
       out[(size_t)y * nz * nx] = __fmul_rn(f, a);
-      prefix = __fadd_rn(prefix, m);
     }
   }
 }
@@ -141,10 +186,15 @@ __global__ void k_reduce_views(const float* __restrict__ part, int nv, int nchun
 // k_rot_adj: grid (nz, nsplit), block kRotAdjThreads.  Accumulates
 // sum_s R'(a_s .* T_s) for the slots of this split into acc (shared or the
 // global per-CTA buffer) and adds/writes it into imgpart[split][z][:][:].
+// CACHED: a_s from the attenuation cache; otherwise rotated mu-map + depth
+// scan per view (imrotate! of the mu-map and the attenuation of
+// src/backproject.jl:285-317).
 constexpr int kRotAdjThreads = 512;
 
+template <bool CACHED>
 __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const float* __restrict__ T,
                                                                 const float* __restrict__ mumap,
+                                                                const float* __restrict__ att,
                                                                 const float4* __restrict__ rot,
                                                                 const int* __restrict__ vidx, int nv,
                                                                 float* __restrict__ imgpart, int accumulate,
@@ -153,6 +203,7 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int z = blockIdx.x, split = blockIdx.y;
   const int slice = nx * ny;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   float* acc;
   float* S;
   float* segsum;
@@ -176,58 +227,70 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
   const int seglen = (ny + nseg - 1) / nseg;
   const int myseg = threadIdx.x / nx, o1s = threadIdx.x - myseg * nx;
   for (int s = s0; s < s1; ++s) {
-    const float4 r = rot[vidx[s]];
+    const int v = vidx[s];
+    const float4 r = rot[v];
     RotPos R{r.x, r.y, g.c0};
     const bool ident = r.z != 0.f;
     __syncthreads();
-    // 1) rotated mu-map of this view on the rotated grid (forward sampling)
-    for (int k = threadIdx.x; k < slice; k += blockDim.x) {
-      int o2 = k / nx, o1 = k - o2 * nx;
-      S[k] = ident ? __ldg(mu + k) : bilinear(mu, nx, R, o1, o2);
-    }
-    __syncthreads();
-    // 2) depth scan along o2 (= y) per column o1, attenuation, times T
-    if (myseg < nseg) {
-      const int ya = myseg * seglen, yb = min(ny, ya + seglen);
-      float sum = 0.f;
-      for (int y = ya; y < yb; ++y) sum = __fadd_rn(sum, S[y * nx + o1s]);
-      segsum[myseg * nx + o1s] = sum;
-    }
-    __syncthreads();
-    if (myseg < nseg) {
-      const int ya = myseg * seglen, yb = min(ny, ya + seglen);
-      float prefix = 0.f;
-      for (int q = 0; q < myseg; ++q) prefix = __fadd_rn(prefix, segsum[q * nx + o1s]);
-      const float* Tc = T + ((size_t)s * ny * nz + z) * nx + o1s;
-      for (int y = ya; y < yb; ++y) {
-        float m = S[y * nx + o1s];
-        float e = __fadd_rn(prefix, __fmul_rn(0.5f, m));
-        float at = expf(__fmul_rn(e, mdy));
-        S[y * nx + o1s] = __fmul_rn(at, __ldg(Tc + (size_t)y * nz * nx));
-        prefix = __fadd_rn(prefix, m);
+    if (CACHED) {
+      // S = a .* T on the rotated grid (coalesced rows of x)
+      const float* av = att + ((size_t)v * ny * nz + z) * nx;
+      const float* tv = T + ((size_t)s * ny * nz + z) * nx;
+      for (int y = warp; y < ny; y += nwarps)
+        for (int x = lane; x < nx; x += 32) {
+          const size_t o = (size_t)y * nz * nx + x;
+          S[y * nx + x] = __fmul_rn(__ldg(av + o), __ldg(tv + o));
+        }
+    } else {
+      // 1) rotated mu-map of this view on the rotated grid (forward sampling)
+      for (int y = warp; y < ny; y += nwarps)
+        for (int x = lane; x < nx; x += 32) S[y * nx + x] = ident ? __ldg(mu + y * nx + x) : bilinear(mu, nx, R, x, y);
+      __syncthreads();
+      // 2) depth scan along y per column x, attenuation, times T
+      if (myseg < nseg) {
+        const int ya = myseg * seglen, yb = min(ny, ya + seglen);
+        float sum = 0.f;
+        for (int y = ya; y < yb; ++y) sum = __fadd_rn(sum, S[y * nx + o1s]);
+        segsum[myseg * nx + o1s] = sum;
+      }
+      __syncthreads();
+      if (myseg < nseg) {
+        const int ya = myseg * seglen, yb = min(ny, ya + seglen);
+        float prefix = 0.f;
+        for (int q = 0; q < myseg; ++q) prefix = __fadd_rn(prefix, segsum[q * nx + o1s]);
+        const float* Tc = T + ((size_t)s * ny * nz + z) * nx + o1s;
+        for (int y = ya; y < yb; ++y) {
+          float m = S[y * nx + o1s];
+          float e = __fadd_rn(prefix, __fmul_rn(0.5f, m));
+          float at = expf(__fmul_rn(e, mdy));
+          S[y * nx + o1s] = __fmul_rn(at, __ldg(Tc + (size_t)y * nz * nx));
+          prefix = __fadd_rn(prefix, m);
+        }
       }
     }
     __syncthreads();
-    // 3) transpose of the bilinear sampling, 9 disjoint lattice classes
+    // 3) transpose of the bilinear sampling: 9 lattice classes (o1 mod 3,
+    //    o2 mod 3); inside a class the 2x2 footprints of two points are >= 2.1
+    //    pixels apart (|Rot (3a,3b)|_inf >= 3/sqrt 2), so they never overlap
     for (int cls = 0; cls < 9; ++cls) {
       const int c1 = cls % 3, c2 = cls / 3;
-      const int n1 = (nx - c1 + 2) / 3, n2 = (ny - c2 + 2) / 3;
-      for (int k = threadIdx.x; k < n1 * n2; k += blockDim.x) {
-        int q2 = k / n1, q1 = k - q2 * n1;
-        int o1 = c1 + 3 * q1, o2 = c2 + 3 * q2;
-        float val = S[o1 + o2 * nx];
-        float s1, s2;
-        R.pos(o1, o2, s1, s2);
-        float f1 = floorf(s1), f2 = floorf(s2);
-        int j1 = (int)f1, j2 = (int)f2;
-        float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
-        float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
-        bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
-        bool y0 = (unsigned)j2 < (unsigned)ny, y1 = (unsigned)(j2 + 1) < (unsigned)ny;
-        if (x0 && y0) acc[j1 + j2 * nx] += __fmul_rn(__fmul_rn(u1, u2), val);
-        if (x1 && y0) acc[j1 + 1 + j2 * nx] += __fmul_rn(__fmul_rn(t1, u2), val);
-        if (x0 && y1) acc[j1 + (j2 + 1) * nx] += __fmul_rn(__fmul_rn(u1, t2), val);
-        if (x1 && y1) acc[j1 + 1 + (j2 + 1) * nx] += __fmul_rn(__fmul_rn(t1, t2), val);
+      for (int o2 = c2 + 3 * warp; o2 < ny; o2 += 3 * nwarps) {
+        for (int o1 = c1 + 3 * lane; o1 < nx; o1 += 96) {
+          const float val = S[o1 + o2 * nx];
+          float s1, s2;
+          R.pos(o1, o2, s1, s2);
+          const float f1 = floorf(s1), f2 = floorf(s2);
+          const int j1 = (int)f1, j2 = (int)f2;
+          const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
+          const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
+          const bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
+          const bool y0 = (unsigned)j2 < (unsigned)ny, y1 = (unsigned)(j2 + 1) < (unsigned)ny;
+          float* a0 = acc + j1 + j2 * nx;
+          if (x0 && y0) a0[0] += __fmul_rn(__fmul_rn(u1, u2), val);
+          if (x1 && y0) a0[1] += __fmul_rn(__fmul_rn(t1, u2), val);
+          if (x0 && y1) a0[nx] += __fmul_rn(__fmul_rn(u1, t2), val);
+          if (x1 && y1) a0[nx + 1] += __fmul_rn(__fmul_rn(t1, t2), val);
+        }
       }
       __syncthreads();
     }

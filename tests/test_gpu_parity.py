@@ -81,3 +81,18 @@ def test_osem_mlem(S, O):
     x0 = np.ones((nx, ny, nz), np.float32, order="F")
     assert relerr(S.mlem(x0, yn, bg, plan, niter=3), G.mlem(x0, yn, bg, 3)) <= TOL
     assert relerr(S.osem(x0, yn, bg, S.Ablock(plan, 4), niter=2), G.osem(x0, yn, bg, 4, 2)) <= TOL
+
+
+@pytest.mark.parametrize("cache", ["0", "1"])
+def test_attenuation_cache_on_off(S, O, cache, monkeypatch):
+    """Same results with the per-plan attenuation cache on and off."""
+    monkeypatch.setenv("SPECT_ATTEN_CACHE", cache)
+    rng = np.random.default_rng(77)
+    nx, nz, nview = 24, 16, 10
+    mumap, psfs = _case(rng, nx, nz, nview, 7, 5, mu_scale=0.03)
+    plan = S.SPECTplan(mumap, psfs, 4.8)
+    G = O.Geometry(mumap, psfs, 4.8)
+    x = np.asfortranarray(rng.random((nx, nx, nz)), np.float32)
+    y = np.asfortranarray(rng.random((nx, nz, nview)), np.float32)
+    assert relerr(S.project(x, plan), G.project(x)) <= TOL
+    assert relerr(S.backproject(y, plan), G.backproject(y)) <= TOL
