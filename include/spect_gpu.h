@@ -97,6 +97,25 @@ int spect_project(spect_plan_t plan, float* views, const float* image, const int
 int spect_project_host(spect_plan_t plan, float* views, const float* image, const int32_t* index,
                        int nindex);
 
+/* Forward projection that allocates nothing (no counterpart in the
+ * reference).  Same result as spect_project, for callers that cannot call
+ * cudaMalloc once their plan exists: processes whose device memory is
+ * reserved up front by another allocator (a serving framework's memory
+ * pool), and real-time acquisition pipelines that forbid allocation after
+ * start-up.  Its scratch (the rotated planes and the depth-chunk partial
+ * views) lives in one file-scope device array of 32 MiB that every GPU
+ * loading this library holds until the process exits; the views are
+ * processed in groups that fit it, and a plan whose single view needs more
+ * (nx*ny*nz + 16*nx*nz floats > 32 MiB) is rejected with
+ * SPECT_ERR_UNSUPPORTED.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  All calls share the array and no part of it needs to
+ * start at zero, but calls that overlap on the GPU (other streams, other
+ * threads) race on it: serialise them.  Device pointers, enqueued on
+ * stream; the plan's device must be the current device. */
+int spect_project_static_scratch(spect_plan_t plan, float* views, const float* image, const int32_t* index,
+                                 int nindex, void* stream);
+
 /* backproject!(image, views, plan; index) (src/backproject.jl:132-162; 340-370
  * in file).  image = sum_i P_{index[i]}' views[i]; image need not be zeroed. */
 int spect_backproject(spect_plan_t plan, float* image, const float* views, const int32_t* index,

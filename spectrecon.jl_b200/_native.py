@@ -24,6 +24,7 @@ _SIGS = {
     "spect_plan_info": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_Z)], _I),
     "spect_project": ([_P, _P, _P, _P, _I, _P], _I),
     "spect_project_host": ([_P, _P, _P, _P, _I], _I),
+    "spect_project_static_scratch": ([_P, _P, _P, _P, _I, _P], _I),
     "spect_backproject": ([_P, _P, _P, _P, _I, _P], _I),
     "spect_backproject_host": ([_P, _P, _P, _P, _I], _I),
     "spect_mlem": ([_P, _P, _P, _P, _P, _I, _P], _I),

@@ -359,12 +359,12 @@ cudaError_t conv_launch(const spect_plan_s* p, int kind, int grid, cudaStream_t 
 
 // forward projection of nidx views (device index list vidx) into views;
 // with y/bg non-null the output is the EM ratio y/(A x + bg).
-int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, int nidx, cudaStream_t st,
-            const float* y, const float* bg) {
+int forward_scratch(spect_plan_s* p, float* views, const float* image, const int* vidx, int nidx, cudaStream_t st,
+                    const float* y, const float* bg, float* Pbuf, float* partbuf, int gmax) {
   const Geom& g = p->g;
   if (p->interp != SPECT_INTERP_TWO) return fail(SPECT_ERR_UNSUPPORTED, "interpmeth :one is not available on the GPU path");
-  for (int g0 = 0; g0 < nidx; g0 += p->gmax) {
-    const int nv = std::min(p->gmax, nidx - g0);
+  for (int g0 = 0; g0 < nidx; g0 += gmax) {
+    const int nv = std::min(gmax, nidx - g0);
     const int* vi = vidx + g0;
     // rotation + attenuation -> P
     int vpb = p->rotf_vpb;
@@ -374,33 +374,38 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
     const float* att = p->d_att;
     LAUNCH(p, K_ROT_FWD, st, "k_rot_fwd",
            if (p->rotf_smem_ok && att) k_rot_fwd<true, true><<<grid, thr, p->rotf_smem, st>>>(
-               g, image, p->d_mumap, att, p->d_rot, vi, nv, p->d_P);
+               g, image, p->d_mumap, att, p->d_rot, vi, nv, Pbuf);
            else if (p->rotf_smem_ok) k_rot_fwd<true, false><<<grid, thr, p->rotf_smem, st>>>(
-               g, image, p->d_mumap, att, p->d_rot, vi, nv, p->d_P);
+               g, image, p->d_mumap, att, p->d_rot, vi, nv, Pbuf);
            else if (att) k_rot_fwd<false, true><<<grid, thr, 0, st>>>(g, image, p->d_mumap, att, p->d_rot, vi, nv,
-                                                                      p->d_P);
+                                                                      Pbuf);
            else k_rot_fwd<false, false><<<grid, thr, 0, st>>>(g, image, p->d_mumap, att, p->d_rot, vi, nv,
-                                                              p->d_P));
+                                                              Pbuf));
     // FFT convolution + depth sum -> part
     Conv2Args a = conv_args(p);
     int cy, nc;
     chunking(p, nv, &cy, &nc);
-    a.P = p->d_P;
+    a.P = Pbuf;
     a.vidx = vi;
     a.nv = nv;
     a.chunkY = cy;
     a.nchunks = nc;
-    a.part = p->d_part;
+    a.part = partbuf;
     int gridc = std::min(p->conv_grid, nv * nc);
     LAUNCH(p, K_CONV_FWD, st, "k_conv_fwd", conv_launch(p, 0, gridc, st, a));
     // chunk sum (+ EM ratio) -> views
     size_t n = (size_t)nv * p->nxz;
     int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16);
     LAUNCH(p, K_REDUCE_VIEWS, st, "k_reduce_views",
-           k_reduce_views<<<rb, 256, 0, st>>>(p->d_part, nv, nc, (int)p->nxz, views + (size_t)g0 * p->nxz, y, bg,
+           k_reduce_views<<<rb, 256, 0, st>>>(partbuf, nv, nc, (int)p->nxz, views + (size_t)g0 * p->nxz, y, bg,
                                               vi));
   }
   return SPECT_OK;
+}
+
+int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, int nidx, cudaStream_t st,
+            const float* y, const float* bg) {
+  return forward_scratch(p, views, image, vidx, nidx, st, y, bg, p->d_P, p->d_part, p->gmax);
 }
 
 // back-projection of nidx views.  mode 0: image = A' views; mode 1: image =
@@ -529,6 +534,33 @@ int run_osem(spect_plan_s* p, float* out, const float* x0, const float* y, const
 int ensure_io(spect_plan_s* p) {
   if (!p->d_io_img) STATUS_TRY(dalloc(p, &p->d_io_img, 2 * p->N));
   if (!p->d_io_views) STATUS_TRY(dalloc(p, &p->d_io_views, 3 * (size_t)p->nview * p->nxz));
+  return SPECT_OK;
+}
+
+// ------------------------------------------------------------------------
+// Scratch of spect_project_static_scratch: a file-scope device array, so the
+// entry point allocates nothing.  Every GPU that loads this library holds it
+// until the process exits.  Host code only sees a stand-in for its name; the
+// device address comes from cudaGetSymbolAddress, once per device.
+constexpr size_t kStaticScratchBytes = (size_t)32 << 20;  // 32 MiB
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+std::mutex g_static_mu;
+void* g_static_ptr[64] = {nullptr};
+
+int static_scratch_address(void** out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SPECT_ERR_UNSUPPORTED, "device index beyond 63");
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(SPECT_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+    g_static_ptr[dev] = ptr;
+  }
+  *out = g_static_ptr[dev];
   return SPECT_OK;
 }
 
@@ -780,6 +812,38 @@ int spect_project(spect_plan_t p, float* views, const float* image, const int32_
   const int* vi;
   STATUS_TRY(stage_index(p, index, nindex, st, &vi));
   return forward(p, views, image, vi, nindex, st, nullptr, nullptr);
+}
+
+int spect_project_static_scratch(spect_plan_t p, float* views, const float* image, const int32_t* index, int nindex,
+                                 void* stream) {
+  if (!p || !views || !image) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev != p->device)
+    return fail(SPECT_ERR_ARG, "spect_project_static_scratch: the plan's device must be the current device");
+  // views per group such that the rotated planes (N floats per view) and the
+  // chunk partials (up to nchunk_max * nz * nx floats per view) fit
+  const size_t per_view = sizeof(float) * (p->N + (size_t)p->nchunk_max * p->nxz) + 512;
+  const size_t G = kStaticScratchBytes / per_view;
+  if (G < 1)
+    return fail(SPECT_ERR_UNSUPPORTED,
+                "spect_project_static_scratch: one view needs " + std::to_string(per_view) +
+                    " bytes of scratch, above the static limit of " + std::to_string(kStaticScratchBytes) + " bytes");
+  void* base = nullptr;
+  STATUS_TRY(static_scratch_address(&base));
+  const int gmax = (int)std::min<size_t>(G, (size_t)p->nview);
+  float* Pbuf = static_cast<float*>(base);
+  size_t off = (sizeof(float) * (size_t)gmax * p->N + 255) & ~(size_t)255;
+  float* partbuf = reinterpret_cast<float*>(static_cast<unsigned char*>(base) + off);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int* vi;
+  STATUS_TRY(stage_index(p, index, nindex, st, &vi));
+  const bool prof = p->prof.on;
+  p->prof.on = false;  // no event creation on this path
+  int rc = forward_scratch(p, views, image, vi, nindex, st, nullptr, nullptr, Pbuf, partbuf, gmax);
+  p->prof.on = prof;
+  return rc;
 }
 
 int spect_project_host(spect_plan_t p, float* views, const float* image, const int32_t* index, int nindex) {
