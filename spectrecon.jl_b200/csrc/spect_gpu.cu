@@ -32,6 +32,7 @@
 
 #include "../../include/spect_gpu.h"
 #include "conv2.cuh"
+#include "rot_one.cuh"
 #include "spect_kernels.cuh"
 
 using namespace spect;
@@ -155,7 +156,14 @@ struct spect_plan_s {
   size_t N = 0, nxz = 0;
   // device
   float* d_mumap = nullptr;
-  float* d_att = nullptr;  // [nview][ny][nz][nx] attenuation cache (optional)
+  float* d_att = nullptr;  // [nview][ny][nz][nx] attenuation cache (optional for :two, required for :one)
+  // :one rotation
+  Rot1Geom r1;
+  Rot1View* d_r1view = nullptr;
+  float* d_R1 = nullptr;       // [gmax][nz][ny][nx] rotated slices / attenuated adjoint planes
+  float* d_gscr_r1 = nullptr;  // per-CTA work grids when they do not fit in shared memory
+  size_t r1f_smem = 0, r1a_smem = 0;
+  int r1f_smem_ok = 1, r1a_smem_ok = 1, r1_grid_y = 1;
   float* d_H = nullptr;
   float4* d_rot = nullptr;
   int* d_viewset = nullptr;
@@ -212,7 +220,7 @@ int dalloc(spect_plan_s* p, T** ptr, size_t count) {
 }
 
 void free_plan(spect_plan_s* p) {
-  void* ptrs[] = {p->d_mumap, p->d_att, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
+  void* ptrs[] = {p->d_mumap, p->d_att, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag,
                   p->d_io_img, p->d_io_views};
@@ -362,7 +370,6 @@ cudaError_t conv_launch(const spect_plan_s* p, int kind, int grid, cudaStream_t 
 int forward_scratch(spect_plan_s* p, float* views, const float* image, const int* vidx, int nidx, cudaStream_t st,
                     const float* y, const float* bg, float* Pbuf, float* partbuf, int gmax) {
   const Geom& g = p->g;
-  if (p->interp != SPECT_INTERP_TWO) return fail(SPECT_ERR_UNSUPPORTED, "interpmeth :one is not available on the GPU path");
   for (int g0 = 0; g0 < nidx; g0 += gmax) {
     const int nv = std::min(gmax, nidx - g0);
     const int* vi = vidx + g0;
@@ -372,6 +379,17 @@ int forward_scratch(spect_plan_s* p, float* views, const float* image, const int
     dim3 grid(g.nz, nsplit);
     const int thr = g.nx * vpb;
     const float* att = p->d_att;
+    if (p->interp == SPECT_INTERP_ONE) {
+      // 3-pass shear rotation of the image slices, then the attenuation
+      dim3 g1(g.nz, std::min(nv, p->r1_grid_y));
+      LAUNCH(p, K_ROT_FWD, st, "k_rot1_fwd",
+             k_rot1_fwd<<<g1, kRot1Threads, p->r1f_smem_ok ? p->r1f_smem : 0, st>>>(
+                 p->r1, image, 0, p->d_r1view, vi, nv, p->d_R1, p->r1f_smem_ok, p->d_gscr_r1));
+      const size_t n = (size_t)nv * p->N;
+      LAUNCH(p, K_ROT_FWD, st, "k_att_combine",
+             k_att_combine<false><<<(int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16), 256, 0, st>>>(
+                 att, p->d_R1, vi, nv, g.nx, g.ny, g.nz, Pbuf));
+    } else
     LAUNCH(p, K_ROT_FWD, st, "k_rot_fwd",
            if (p->rotf_smem_ok && att) k_rot_fwd<true, true><<<grid, thr, p->rotf_smem, st>>>(
                g, image, p->d_mumap, att, p->d_rot, vi, nv, Pbuf);
@@ -413,7 +431,6 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
 int backward(spect_plan_s* p, float* image, const float* views, const int* vidx, int nidx, cudaStream_t st,
              int mode, const float* asum) {
   const Geom& g = p->g;
-  if (p->interp != SPECT_INTERP_TWO) return fail(SPECT_ERR_UNSUPPORTED, "interpmeth :one is not available on the GPU path");
   const int nsplit = p->nsplit_adj;
   if (nidx == 0) {
     CUDA_TRY(cudaMemsetAsync(p->d_imgpart, 0, sizeof(float) * p->N * nsplit, st));
@@ -436,6 +453,15 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj", conv_launch(p, 1, std::min(p->conv_grid, nv * nc), st, a));
     dim3 grid(g.nz, nsplit);
     const size_t rsm = p->rota_smem_ok ? p->rota_smem : 0;
+    if (p->interp == SPECT_INTERP_ONE) {
+      const size_t n = (size_t)nv * p->N;
+      LAUNCH(p, K_ROT_ADJ, st, "k_att_combine",
+             k_att_combine<true><<<(int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16), 256, 0, st>>>(
+                 p->d_att, p->d_P, vi, nv, g.nx, g.ny, g.nz, p->d_R1));
+      LAUNCH(p, K_ROT_ADJ, st, "k_rot1_adj",
+             k_rot1_adj<<<grid, kRot1Threads, p->r1a_smem_ok ? p->r1a_smem : 0, st>>>(
+                 p->r1, p->d_R1, p->d_r1view, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->r1a_smem_ok, p->d_gscr_r1));
+    } else
     LAUNCH(p, K_ROT_ADJ, st, "k_rot_adj",
            if (p->d_att) k_rot_adj<true><<<grid, kRotAdjThreads, rsm, st>>>(
                g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
@@ -649,7 +675,11 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
       fr = 0;
     }
     bool want = !(env && env[0] == '0') && need <= std::min(fr / 4, (size_t)32 << 30);
-    if (want && dalloc(p, &p->d_att, p->N * (size_t)nview) != SPECT_OK) {
+    if (interpmeth == SPECT_INTERP_ONE) {
+      // the :one path reads its attenuation from the cache
+      int st1 = dalloc(p, &p->d_att, p->N * (size_t)nview);
+      if (st1 != SPECT_OK) return bail(st1);
+    } else if (want && dalloc(p, &p->d_att, p->N * (size_t)nview) != SPECT_OK) {
       p->d_att = nullptr;
       g_err.clear();
     }
@@ -718,7 +748,74 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
       (st = up(p->d_all, all.data(), sizeof(int) * nview)))
     return bail(st);
 
-  if (p->d_att) {
+  if (interpmeth == SPECT_INTERP_ONE) {
+    // Rot1 geometry and per-view shear parameters (src/rotatez.jl:249-272)
+    const int pad1 = (int)std::ceil(1.0 + nx * std::sqrt(2.0) / 2.0 - nx / 2.0);
+    p->r1 = Rot1Geom{nx, ny, nz, nx + 2 * pad1, pad1, nx + 2 * pad1 + 1};
+    const int L = p->r1.L;
+    p->r1f_smem = sizeof(float) * ((size_t)p->r1.LS * L + (size_t)kRot1Warps * L);
+    p->r1a_smem = p->r1f_smem + sizeof(float) * (size_t)nx * nx;
+    p->r1f_smem_ok = p->r1f_smem <= p->max_smem;
+    p->r1a_smem_ok = p->r1a_smem <= p->max_smem;
+    if (p->r1f_smem_ok &&
+        cudaFuncSetAttribute((const void*)k_rot1_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)p->r1f_smem) != cudaSuccess)
+      return bail(fail(SPECT_ERR_CUDA, "k_rot1_fwd shared memory"));
+    if (p->r1a_smem_ok &&
+        cudaFuncSetAttribute((const void*)k_rot1_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)p->r1a_smem) != cudaSuccess)
+      return bail(fail(SPECT_ERR_CUDA, "k_rot1_adj shared memory"));
+    p->r1_grid_y = std::max(1, cdiv(4 * p->sm_count, nz));
+    size_t gs = 0;
+    if (!p->r1f_smem_ok) gs = std::max(gs, (size_t)nz * p->r1_grid_y * (p->r1f_smem / sizeof(float)));
+    if (!p->r1a_smem_ok) gs = std::max(gs, (size_t)nz * p->nsplit_adj * (p->r1a_smem / sizeof(float)));
+    if (gs && (st = dalloc(p, &p->d_gscr_r1, gs))) return bail(st);
+    if ((st = dalloc(p, &p->d_R1, (size_t)p->gmax * p->N)) || (st = dalloc(p, &p->d_r1view, nview)))
+      return bail(st);
+    std::vector<Rot1View> rv(nview);
+    const double kHalfPi = 1.5707963267948966;
+    const double rtol = 3.4526698300124393e-4;  // sqrt(eps(Float32)): isapprox default for a Float32 angle
+    for (int v = 0; v < nview; ++v) {
+      const double th = (double)p->angles[v];
+      Rot1View r{0.0, 0.0, 0, 2};
+      if (std::fmod(th, kTwoPi) == 0.0) {
+        r.mode = 0;
+      } else {
+        long fl = (long)std::floor(0.5 + th / kHalfPi);
+        r.m = (int)(((fl % 4) + 4) % 4);
+        const double mh = r.m * kHalfPi;
+        if (std::fabs(th - mh) <= rtol * std::max(std::fabs(th), std::fabs(mh))) {
+          r.mode = 1;
+        } else {
+          const double mt = th - mh;
+          r.tn = std::tan(mt / 2);
+          r.sn = -std::sin(mt);
+        }
+      }
+      rv[v] = r;
+    }
+    if ((st = up(p->d_r1view, rv.data(), sizeof(Rot1View) * nview))) return bail(st);
+  }
+
+  if (p->d_att && interpmeth == SPECT_INTERP_ONE) {
+    // :one-rotated mu-map per group of views, then the depth scan
+    cudaError_t e = cudaSuccess;
+    for (int v0 = 0; v0 < nview && e == cudaSuccess; v0 += p->gmax) {
+      const int nv = std::min(p->gmax, nview - v0);
+      dim3 g1(nz, std::min(nv, p->r1_grid_y));
+      k_rot1_fwd<<<g1, kRot1Threads, p->r1f_smem_ok ? p->r1f_smem : 0>>>(
+          p->r1, p->d_mumap, 0, p->d_r1view, p->d_all + v0, nv, p->d_R1, p->r1f_smem_ok, p->d_gscr_r1);
+      const size_t n = (size_t)nv * nz * nx;
+      k_att_scan<<<(int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16), 256>>>(
+          p->d_R1, nv, nx, ny, nz, dy, p->d_att + (size_t)v0 * p->N);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+      fail(SPECT_ERR_CUDA, std::string("attenuation cache (:one): ") + cudaGetErrorString(e));
+      return bail(SPECT_ERR_CUDA);
+    }
+  } else if (p->d_att) {
     dim3 grid(nz, std::max(1, std::min(cdiv(2 * p->sm_count, nz), cdiv(nview, p->rotf_vpb))));
     const int thr = nx * p->rotf_vpb;
     if (p->att_smem_ok)

@@ -78,3 +78,15 @@ def test_full_c2_subset_osem_update(S, O):
 
     b = G.osem(x0, st.ynoisy, st.background, 8, 1)
     assert relerr(a, b) <= TOL
+
+
+def test_config_parity_one(S, O):
+    """interpmeth :one at the single larger study's sizes (256x128 padded planes, L = 184)."""
+    st = _study(S, 128, 80, 120, 37, 6.0, (0.0096, 0.015), seed=9)
+    plan = S.SPECTplan(st.mumap, st.psfs, st.dy, interpmeth="one")
+    G = O.Geometry(st.mumap, st.psfs, st.dy, interp="one")
+    idx = np.array([0, 30, 45, 77], np.int32)  # includes 90 degrees (view 30 of 120)
+    assert relerr(S.project(st.image, plan, index=idx), G.project(st.image, index=idx)) <= TOL
+    rng = np.random.default_rng(3)
+    y = np.asfortranarray(rng.random((128, 80, len(idx))), np.float32)
+    assert relerr(S.backproject(y, plan, index=idx), G.backproject(y, index=idx)) <= TOL

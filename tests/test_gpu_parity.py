@@ -22,25 +22,28 @@ def _case(rng, nx, nz, nview, px, pz, mu_scale=1.0):
     return mumap, psfs
 
 
-@pytest.mark.parametrize("nx,nz,nview,px,pz", [(8, 6, 7, 5, 3), (32, 20, 30, 5, 3), (20, 14, 9, 7, 5)])
-def test_project_backproject_small(S, O, nx, nz, nview, px, pz):
+@pytest.mark.parametrize("interp", ["two", "one"])
+@pytest.mark.parametrize("nx,nz,nview,px,pz", [(8, 6, 7, 5, 3), (32, 20, 30, 5, 3), (20, 14, 9, 7, 5), (16, 10, 8, 3, 3)])
+def test_project_backproject_small(S, O, nx, nz, nview, px, pz, interp):
+    """nview = 8 puts views at exact multiples of 90 degrees (the rot_f90-only branch of :one)."""
     rng = np.random.default_rng(nx * 100 + nz)
     mumap, psfs = _case(rng, nx, nz, nview, px, pz, mu_scale=0.02)
     dy = 4.7952
-    plan = S.SPECTplan(mumap, psfs, dy)
-    G = O.Geometry(mumap, psfs, dy)
+    plan = S.SPECTplan(mumap, psfs, dy, interpmeth=interp)
+    G = O.Geometry(mumap, psfs, dy, interp=interp)
     x = np.asfortranarray(rng.random((nx, nx, nz)), np.float32)
     y = np.asfortranarray(rng.random((nx, nz, nview)), np.float32)
     assert relerr(S.project(x, plan), G.project(x)) <= TOL
     assert relerr(S.backproject(y, plan), G.backproject(y)) <= TOL
 
 
-def test_dot_adjoint_32(S):
+@pytest.mark.parametrize("interp", ["two", "one"])
+def test_dot_adjoint_32(S, interp):
     """<y, A x> == <x, A' y> (test/adjoint-project.jl:52-106)."""
     rng = np.random.default_rng(52)
     nx, nz, nview = 32, 20, 30
     mumap, psfs = _case(rng, nx, nz, nview, 5, 3)
-    plan = S.SPECTplan(mumap, psfs, 4.7952)
+    plan = S.SPECTplan(mumap, psfs, 4.7952, interpmeth=interp)
     x = np.asfortranarray(rng.standard_normal((nx, nx, nz)), np.float32)
     y = np.asfortranarray(rng.standard_normal((nx, nz, nview)), np.float32)
     a = np.dot(y.ravel().astype(np.float64), S.project(x, plan).ravel().astype(np.float64))
