@@ -151,6 +151,24 @@ int spect_em_subset_update(spect_plan_t plan, float* x, const float* ynoisy, con
 int spect_subset_sensitivity(spect_plan_t plan, float* asum, const int32_t* index, int nindex,
                              void* stream);
 
+/* Batched OS-EM (no counterpart in the reference: its osem! runs one
+ * reconstruction at a time).  A batch holds njobs plans of any sizes (each
+ * plan at most once) with their subset counts and iteration counts.  Every
+ * job's whole osem! (sensitivities, then niter x nblocks fused subset
+ * updates) is enqueued on its own stream and captured once into a single
+ * CUDA graph; spect_batch_run launches that graph on `stream` (one launch
+ * for all reconstructions; the jobs overlap on the GPU).  set_job gives the
+ * device buffers of job j (out, x0 [nz][ny][nx]; ynoisy, background
+ * [nview][nz][nx]) and checks background > 0 (synchronously); changing a
+ * job's buffers re-captures the graph at the next run. */
+typedef struct spect_batch_s* spect_batch_t;
+int spect_batch_create(spect_batch_t* batch, int njobs, const spect_plan_t* plans, const int* nblocks,
+                       const int* niter);
+int spect_batch_set_job(spect_batch_t batch, int job, float* out, const float* x0, const float* ynoisy,
+                        const float* background);
+int spect_batch_run(spect_batch_t batch, void* stream);
+int spect_batch_destroy(spect_batch_t batch);
+
 /* Kernel accounting (no counterpart in the reference; measurement support).
  * spect_kernel_launches: number of kernels this library has launched in the
  * process.  spect_plan_profile(plan, on): when on, every kernel the plan

@@ -36,7 +36,7 @@ from . import _native
 from ._native import SpectError, check
 
 __all__ = [
-    "SPECTplan", "project", "project_", "backproject", "backproject_", "mlem", "mlem_", "osem", "osem_",
+    "Batch", "SPECTplan", "project", "project_", "backproject", "backproject_", "mlem", "mlem_", "osem", "osem_",
     "Ablock", "psf_gauss", "nthreads", "SpectError",
 ]
 
@@ -310,6 +310,50 @@ def osem(x0, ynoisy, background, Ab: Ablock, niter=16, chat=False):
     """osem(x0, ynoisy, background, Ab; niter) (src/ml-os-em.jl:143)."""
     out = np.empty(Ab.plan.imgsize, dtype=np.float32, order="F")
     return osem_(out, x0, ynoisy, background, Ab, niter=niter, chat=chat)
+
+
+class Batch:
+    """Many OS-EM reconstructions of uneven sizes run as ONE CUDA-graph launch.
+
+    ``Batch(plans, nblocks, niter)``; ``set_job(j, out, x0, ynoisy, background)``
+    with device arrays (column-major like the reference); ``run(stream)``
+    enqueues the whole batch (every job's osem!, src/ml-os-em.jl:97-131) as
+    one graph launch.  No counterpart in the reference (one osem! at a time).
+    """
+
+    def __init__(self, plans, nblocks, niter):
+        self.plans = list(plans)
+        n = len(self.plans)
+        nb = np.ascontiguousarray(np.broadcast_to(np.asarray(nblocks, np.int32), (n,)))
+        ni = np.ascontiguousarray(np.broadcast_to(np.asarray(niter, np.int32), (n,)))
+        self.nblocks, self.niter = nb, ni
+        hs = (ctypes.c_void_p * n)(*[p.handle for p in self.plans])
+        h = ctypes.c_void_p()
+        check(_native.lib().spect_batch_create(ctypes.byref(h), n, hs, _ptr(nb), _ptr(ni)))
+        self._h = h
+        self._keep = {}
+
+    def set_job(self, j, out, x0, ynoisy, background):
+        p = self.plans[j]
+        V = _views_shape(p, p.nview)
+        ptrs = (_dev_ptr(out, p.imgsize, "out"), _dev_ptr(x0, p.imgsize, "x0"), _dev_ptr(ynoisy, V, "ynoisy"),
+                _dev_ptr(background, V, "background"))
+        self._keep[j] = (out, x0, ynoisy, background)
+        check(_native.lib().spect_batch_set_job(self._h, int(j), *ptrs))
+
+    def run(self, stream=None):
+        check(_native.lib().spect_batch_run(self._h, _stream_ptr(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _native.lib().spect_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def psf_gauss(ny=128, px=11, pz=None, fwhm_start=1, fwhm_end=4, fwhm=None, fwhm_x=None, fwhm_z=None,

@@ -42,12 +42,17 @@ cudaError_t SPECT_CAT(conv2_launch_rx, SPECT_RX)(int kind, int RZ, int grid, siz
   return cudaLaunchKernel(k, dim3(grid), dim3(kConvThreads), params, smem, st);
 }
 
+// The attribute is set to the device's opt-in maximum (plans of different
+// sizes share the instantiation; each launch passes its own size).
 cudaError_t SPECT_CAT(conv2_setup_rx, SPECT_RX)(int RZ, size_t smem, int* occ) {
-  int o = 64;
+  int o = 64, dev = 0, optin = 0;
+  cudaError_t e0 = cudaGetDevice(&dev);
+  if (e0 == cudaSuccess) e0 = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e0 != cudaSuccess) return e0;
   for (int kind = 0; kind < 3; ++kind) {
     const void* k = kernel_ptr_rt(kind, RZ);
     if (!k) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     if (e != cudaSuccess) return e;
     int b = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k, kConvThreads, smem);

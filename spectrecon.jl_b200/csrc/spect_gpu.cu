@@ -184,6 +184,8 @@ struct spect_plan_s {
   float* d_ones = nullptr;       // [nview][nz][nx]
   float* d_asum = nullptr;       // [nblocks][N]
   int asum_blocks = 0;
+  int* d_sub = nullptr;          // [nview] subset view table of the last prepared nblocks
+  int sub_nblocks = 0;
   int* d_flag = nullptr;
   // host-call staging (lazily allocated)
   float* d_io_img = nullptr;   // [2][N]
@@ -222,7 +224,7 @@ int dalloc(spect_plan_s* p, T** ptr, size_t count) {
 void free_plan(spect_plan_s* p) {
   void* ptrs[] = {p->d_mumap, p->d_att, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
-                  p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag,
+                  p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
                   p->d_io_img, p->d_io_views};
   for (void* q : ptrs)
     if (q) cudaFree(q);
@@ -308,23 +310,22 @@ int configure(spect_plan_s* p) {
   p->rotf_smem = (p->d_att ? 1 : 2) * slice * sizeof(float);
   p->rotf_smem_ok = p->rotf_smem <= p->max_smem;
   if (p->rotf_smem_ok) {
-    const void* kf = p->d_att ? (const void*)k_rot_fwd<true, true> : (const void*)k_rot_fwd<true, false>;
-    CUDA_TRY(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->rotf_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_fwd<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)p->max_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_fwd<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)p->max_smem));
   }
   p->att_smem_ok = slice * sizeof(float) <= p->max_smem;
   if (p->att_smem_ok)
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_atten_build<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(slice * sizeof(float))));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_atten_build<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
   // ---- adjoint rotation
   int nseg = std::max(1, kRotAdjThreads / g.nx);
   p->rota_smem = (2 * slice + (size_t)nseg * g.nx) * sizeof(float);
   p->rota_smem_ok = p->rota_smem <= p->max_smem;
   p->nsplit_adj = std::max(1, std::min(8, cdiv(2 * p->sm_count, g.nz)));
   if (p->rota_smem_ok) {
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)p->rota_smem));
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)p->rota_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
   } else {
     size_t per = 2 * slice + (size_t)nseg * g.nx;
     STATUS_TRY(dalloc(p, &p->d_gscr_adj, per * g.nz * p->nsplit_adj));
@@ -533,28 +534,49 @@ int check_background(spect_plan_s* p, const float* bg, cudaStream_t st) {
 }
 
 // OS-EM on device buffers (mlem = one block)
-int run_osem(spect_plan_s* p, float* out, const float* x0, const float* y, const float* bg, int nblocks, int niter,
-             cudaStream_t st) {
+// Host-side preparation of OS-EM with nblocks subsets (Ablock,
+// src/ml-os-em.jl:70-84): validation, EM buffers, and the device table of
+// the subsets' views (subset b = views b, b+nblocks, ... , 0-based) in
+// p->d_sub.  Synchronous; nothing of it may run during a stream capture.
+int prepare_osem(spect_plan_s* p, int nblocks, int niter) {
   if (nblocks < 1 || p->nview % nblocks != 0) return fail(SPECT_ERR_NBLOCKS, "nview must be divisible by nblocks!");
   if (niter < 0) return fail(SPECT_ERR_ARG, "niter must be >= 0");
   STATUS_TRY(ensure_em(p, nblocks));
-  STATUS_TRY(check_background(p, bg, st));
+  if (!p->d_sub) STATUS_TRY(dalloc(p, &p->d_sub, p->nview));
+  if (p->sub_nblocks != nblocks) {
+    const int nsub = p->nview / nblocks;
+    std::vector<int> idx(p->nview);
+    for (int b = 0; b < nblocks; ++b)
+      for (int s = 0; s < nsub; ++s) idx[(size_t)b * nsub + s] = b + s * nblocks;
+    CUDA_TRY(cudaMemcpy(p->d_sub, idx.data(), sizeof(int) * p->nview, cudaMemcpyHostToDevice));
+    p->sub_nblocks = nblocks;
+  }
+  return SPECT_OK;
+}
+
+// OS-EM enqueued on st only (no host synchronisation or host staging, so it
+// can be captured into a CUDA graph); needs prepare_osem(p, nblocks) first.
+int enqueue_osem(spect_plan_s* p, float* out, const float* x0, const float* y, const float* bg, int nblocks, int niter,
+                 cudaStream_t st) {
   const int nsub = p->nview / nblocks;
-  std::vector<int> idx(p->nview);
   for (int b = 0; b < nblocks; ++b)
-    for (int s = 0; s < nsub; ++s) idx[(size_t)b * nsub + s] = b + s * nblocks;
-  CUDA_TRY(cudaMemcpyAsync(p->d_idx, idx.data(), sizeof(int) * p->nview, cudaMemcpyHostToDevice, st));
-  for (int b = 0; b < nblocks; ++b)
-    STATUS_TRY(backward(p, p->d_asum + (size_t)b * p->N, p->d_ones, p->d_idx + (size_t)b * nsub, nsub, st, 1,
+    STATUS_TRY(backward(p, p->d_asum + (size_t)b * p->N, p->d_ones, p->d_sub + (size_t)b * nsub, nsub, st, 1,
                         nullptr));
   if (out != x0) CUDA_TRY(cudaMemcpyAsync(out, x0, sizeof(float) * p->N, cudaMemcpyDeviceToDevice, st));
   for (int it = 0; it < niter; ++it)
     for (int b = 0; b < nblocks; ++b) {
-      const int* vi = p->d_idx + (size_t)b * nsub;
+      const int* vi = p->d_sub + (size_t)b * nsub;
       STATUS_TRY(forward(p, p->d_views_tmp, out, vi, nsub, st, y, bg));
       STATUS_TRY(backward(p, out, p->d_views_tmp, vi, nsub, st, 2, p->d_asum + (size_t)b * p->N));
     }
   return SPECT_OK;
+}
+
+int run_osem(spect_plan_s* p, float* out, const float* x0, const float* y, const float* bg, int nblocks, int niter,
+             cudaStream_t st) {
+  STATUS_TRY(prepare_osem(p, nblocks, niter));
+  STATUS_TRY(check_background(p, bg, st));
+  return enqueue_osem(p, out, x0, y, bg, nblocks, niter, st);
 }
 
 int ensure_io(spect_plan_s* p) {
@@ -590,6 +612,78 @@ int static_scratch_address(void** out) {
   return SPECT_OK;
 }
 
+}  // namespace
+
+// ------------------------------------------------------------------------
+// Batched OS-EM: many reconstructions (one plan each, uneven sizes) enqueued
+// on one non-blocking stream per job and captured into a single CUDA graph;
+// spect_batch_run launches that graph once.
+struct spect_batch_s {
+  std::vector<spect_plan_s*> plans;
+  std::vector<int> nblocks, niter;
+  std::vector<float*> out;
+  std::vector<const float*> x0, y, bg;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> done;
+  cudaStream_t root = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long nkernels = 0;  // kernels in the graph
+  bool dirty = true;
+  std::mutex mu;
+};
+
+namespace {
+void batch_release_graph(spect_batch_s* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+int batch_capture(spect_batch_s* b) {
+  batch_release_graph(b);
+  const int nj = (int)b->plans.size();
+  for (int j = 0; j < nj; ++j)
+    if (!b->out[j] || !b->x0[j] || !b->y[j] || !b->bg[j])
+      return fail(SPECT_ERR_ARG, "spect_batch_run: job " + std::to_string(j) + " has no data");
+  std::vector<char> prof(nj);
+  for (int j = 0; j < nj; ++j) {
+    prof[j] = b->plans[j]->prof.on;
+    b->plans[j]->prof.on = false;  // no event bracketing inside the graph
+  }
+  CUDA_TRY(cudaStreamBeginCapture(b->root, cudaStreamCaptureModeThreadLocal));
+  const unsigned long long l0 = g_launches.load();
+  int rc = SPECT_OK;
+  cudaError_t e = cudaEventRecord(b->fork, b->root);
+  for (int j = 0; j < nj && rc == SPECT_OK && e == cudaSuccess; ++j) {
+    e = cudaStreamWaitEvent(b->streams[j], b->fork, 0);
+    if (e != cudaSuccess) break;
+    rc = enqueue_osem(b->plans[j], b->out[j], b->x0[j], b->y[j], b->bg[j], b->nblocks[j], b->niter[j],
+                      b->streams[j]);
+    if (rc == SPECT_OK) e = cudaEventRecord(b->done[j], b->streams[j]);
+    if (rc == SPECT_OK && e == cudaSuccess) e = cudaStreamWaitEvent(b->root, b->done[j], 0);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(b->root, &g);
+  // captured kernels are counted when the graph runs, not here
+  b->nkernels = g_launches.load() - l0;
+  g_launches.fetch_sub(b->nkernels);
+  for (int j = 0; j < nj; ++j) b->plans[j]->prof.on = prof[j];
+  if (rc != SPECT_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return fail(SPECT_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  b->graph = g;
+  CUDA_TRY(cudaGraphInstantiate(&b->exec, g, 0));
+  b->dirty = false;
+  return SPECT_OK;
+}
 }  // namespace
 
 // ====================================================================== ABI
@@ -758,12 +852,10 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
     p->r1f_smem_ok = p->r1f_smem <= p->max_smem;
     p->r1a_smem_ok = p->r1a_smem <= p->max_smem;
     if (p->r1f_smem_ok &&
-        cudaFuncSetAttribute((const void*)k_rot1_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)p->r1f_smem) != cudaSuccess)
+        cudaFuncSetAttribute((const void*)k_rot1_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem) != cudaSuccess)
       return bail(fail(SPECT_ERR_CUDA, "k_rot1_fwd shared memory"));
     if (p->r1a_smem_ok &&
-        cudaFuncSetAttribute((const void*)k_rot1_adj, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)p->r1a_smem) != cudaSuccess)
+        cudaFuncSetAttribute((const void*)k_rot1_adj, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem) != cudaSuccess)
       return bail(fail(SPECT_ERR_CUDA, "k_rot1_adj shared memory"));
     p->r1_grid_y = std::max(1, cdiv(4 * p->sm_count, nz));
     size_t gs = 0;
@@ -1039,6 +1131,90 @@ int spect_subset_sensitivity(spect_plan_t p, float* asum, const int32_t* index, 
   const int* vi;
   STATUS_TRY(stage_index(p, index, nindex, st, &vi));
   return backward(p, asum, p->d_ones, vi, nindex, st, 1, nullptr);
+}
+
+int spect_batch_create(spect_batch_t* out, int njobs, const spect_plan_t* plans, const int* nblocks,
+                       const int* niter) {
+  if (!out || !plans || !nblocks || !niter || njobs < 1) return fail(SPECT_ERR_ARG, "bad spect_batch_create arguments");
+  *out = nullptr;
+  for (int j = 0; j < njobs; ++j) {
+    if (!plans[j]) return fail(SPECT_ERR_ARG, "null plan in batch");
+    for (int k = 0; k < j; ++k)
+      if (plans[k] == plans[j]) return fail(SPECT_ERR_ARG, "a plan may appear only once in a batch");
+  }
+  spect_batch_s* b = new spect_batch_s;
+  auto bail = [&](int st) {
+    spect_batch_destroy(b);
+    return st;
+  };
+  b->plans.assign(plans, plans + njobs);
+  b->nblocks.assign(nblocks, nblocks + njobs);
+  b->niter.assign(niter, niter + njobs);
+  b->out.assign(njobs, nullptr);
+  b->x0.assign(njobs, nullptr);
+  b->y.assign(njobs, nullptr);
+  b->bg.assign(njobs, nullptr);
+  for (int j = 0; j < njobs; ++j) {
+    std::lock_guard<std::mutex> lk(b->plans[j]->mu);
+    int st = prepare_osem(b->plans[j], nblocks[j], niter[j]);
+    if (st != SPECT_OK) return bail(st);
+  }
+  if (cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(SPECT_ERR_CUDA, "batch stream/event creation"));
+  b->streams.assign(njobs, nullptr);
+  b->done.assign(njobs, nullptr);
+  for (int j = 0; j < njobs; ++j)
+    if (cudaStreamCreateWithFlags(&b->streams[j], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done[j], cudaEventDisableTiming) != cudaSuccess)
+      return bail(fail(SPECT_ERR_CUDA, "batch stream/event creation"));
+  *out = b;
+  return SPECT_OK;
+}
+
+int spect_batch_set_job(spect_batch_t b, int job, float* out, const float* x0, const float* ynoisy,
+                        const float* background) {
+  if (!b || job < 0 || job >= (int)b->plans.size() || !out || !x0 || !ynoisy || !background)
+    return fail(SPECT_ERR_ARG, "bad spect_batch_set_job arguments");
+  std::lock_guard<std::mutex> lk(b->mu);
+  spect_plan_s* p = b->plans[job];
+  {
+    std::lock_guard<std::mutex> lp(p->mu);
+    STATUS_TRY(check_background(p, background, 0));
+  }
+  b->out[job] = out;
+  b->x0[job] = x0;
+  b->y[job] = ynoisy;
+  b->bg[job] = background;
+  b->dirty = true;
+  return SPECT_OK;
+}
+
+int spect_batch_run(spect_batch_t b, void* stream) {
+  if (!b) return fail(SPECT_ERR_ARG, "null batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  if (b->dirty) {
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (auto* p : b->plans) locks.emplace_back(p->mu);
+    STATUS_TRY(batch_capture(b));
+  }
+  CUDA_TRY(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  g_launches.fetch_add(b->nkernels, std::memory_order_relaxed);
+  return SPECT_OK;
+}
+
+int spect_batch_destroy(spect_batch_t b) {
+  if (!b) return fail(SPECT_ERR_ARG, "null batch");
+  cudaDeviceSynchronize();
+  batch_release_graph(b);
+  for (auto s : b->streams)
+    if (s) cudaStreamDestroy(s);
+  for (auto e : b->done)
+    if (e) cudaEventDestroy(e);
+  if (b->root) cudaStreamDestroy(b->root);
+  if (b->fork) cudaEventDestroy(b->fork);
+  delete b;
+  return SPECT_OK;
 }
 
 unsigned long long spect_kernel_launches(void) { return g_launches.load(); }
