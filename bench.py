@@ -266,9 +266,10 @@ def run_ours(args):
                 "flops_per_launch": flops_launch, "avg_launch_ms": round(avg_ms, 4),
                 "kernel_ms_per_step": {k: round(v / args.steps, 3) for k, v in kms.items()},
                 "kernel_launches_per_step": {k: int(v // args.steps) for k, v in kn.items()}}
-    batched = None
+    batched = served = None
     if not args.no_extras:
         batched = run_batched(S, torch)
+        served = run_served(S, njobs=args.served_jobs, rate=args.served_rate)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(st, sample_subsets=args.cpu_subsets)
@@ -283,7 +284,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(4 * nx * ny * nz), "ms_per_step": round(e2e_ms / e2e_steps, 3),
                 "max_rel_diff_vs_device_path": rel},
         "gpu_launches": int(launches), "roofline": roofline, "clocks": clk.summary(),
-        "cpu_baseline": cpu, "batched": batched,
+        "cpu_baseline": cpu, "batched": batched, "served": served,
     }
     if rank == 0:
         print(json.dumps(res), flush=True)
@@ -378,6 +379,85 @@ def run_batched(S, torch, njobs=32, timed_runs=2, plain_sample=6, seed=3):
             "plain_percall_recons_per_s": round(plain, 3), "plain_sample_jobs": len(t_plain),
             "speedup_vs_plain": round(batched / plain, 2), "graph_kernels": int(launches),
             "max_rel_diff_vs_plain": rel}
+
+
+def run_served(S, njobs=500, rate=16.0, big_fraction=0.1, seed=4, pool_small=36, pool_big=3, plain_sample=10,
+               saturated_jobs=150):
+    """Serving configuration: a Poisson stream of reconstruction requests (the
+    batching size mix plus big_fraction of 256x256x128 jobs, 4 OS-EM iterations
+    each) submitted to the continuous-batching server at `rate` per second;
+    p50/p99 submit-to-finish latency and throughput, a saturated run (all
+    requests at once), and the plain per-call path on a sample of the mix."""
+    from importlib import import_module
+
+    W = import_module("spectrecon_b200.workloads")
+    rng = np.random.default_rng(seed)
+    mix = W.batch_mix(pool_small, seed)
+    big = [dict(nx=256, nz=128, nview=int(rng.choice([60, 90, 120, 128])), p=int(rng.choice([11, 21, 37])),
+                k=int(rng.integers(4, 13)), mu_values=(0.0096,), niter=4, seed=seed * 7919 + i) for i in range(pool_big)]
+    for b in big:
+        b["fwhm_end"] = b["p"] / 6.0
+        b["nblocks"] = int(rng.choice(W.divisors_in(b["nview"])))
+    pool = []
+    for j in mix + big:
+        st = W.make_study("c4", nx=j["nx"], nz=j["nz"], nview=j["nview"], p=j["p"], fwhm_end=j["fwhm_end"],
+                          k=j["k"], mu_values=j["mu_values"], nblocks=j["nblocks"], niter=j["niter"], seed=j["seed"])
+        plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+        ytrue = S.project(st.image, plan).astype(np.float64)
+        plan.close()
+        bgv = 0.05 * ytrue.mean()
+        st.background = np.asfortranarray(np.full(ytrue.shape, bgv), np.float32)
+        st.meta["ytrue"] = ytrue
+        pool.append(st)
+    nsm = len(mix)
+    picks = [int(rng.integers(nsm, len(pool))) if rng.uniform() < big_fraction else int(rng.integers(0, nsm))
+             for _ in range(max(njobs, saturated_jobs))]
+    ys = [np.asfortranarray(rng.poisson(pool[k].meta["ytrue"] + pool[k].background), np.float32) for k in picks]
+
+    def stream(n, lam):
+        srv = S.Server(max_active=24)
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, n)) if lam else np.zeros(n)
+        tickets = []
+        t0 = time.perf_counter()
+        for i in range(n):
+            while time.perf_counter() - t0 < arrivals[i]:
+                time.sleep(min(0.002, max(0.0, arrivals[i] - (time.perf_counter() - t0))))
+            st = pool[picks[i]]
+            tickets.append(srv.submit(st.mumap, st.psfs, st.dy, ys[i], st.background, st.nblocks, st.niter))
+        lat = [srv.wait(t)[1] for t in tickets]
+        wall = time.perf_counter() - t0
+        stats = srv.stats()
+        srv.close()
+        return lat, wall, stats
+
+    lat, wall, stats = stream(njobs, rate)
+    slat, swall, sstats = stream(saturated_jobs, None)
+    # plain per-call path on a sample with the same share of big jobs
+    nbig = max(1, int(round(plain_sample * big_fraction)))
+    sample = [k for k in picks if k < nsm][: plain_sample - nbig] + [k for k in picks if k >= nsm][:nbig]
+    t_plain = 0.0
+    for k in sample:
+        st = pool[k]
+        plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+        x0 = np.ones(st.image.shape, np.float32, order="F")
+        y = np.asfortranarray(rng.poisson(st.meta["ytrue"] + st.background), np.float32)
+        t0 = time.perf_counter()
+        plain_osem(S, plan, x0, y, st.background, st.nblocks, st.niter)
+        t_plain += time.perf_counter() - t0
+        plan.close()
+    plain = len(sample) / t_plain
+    served = njobs / wall
+    return {"requests": njobs, "arrival_rate_per_s": rate, "big_fraction": big_fraction,
+            "recons_per_s": round(served, 3), "p50_ms": round(float(np.percentile(lat, 50)), 1),
+            "p99_ms": round(float(np.percentile(lat, 99)), 1), "max_active": int(stats["max_active_seen"]),
+            "failed": int(stats["failed"]),
+            "saturated": {"requests": saturated_jobs, "recons_per_s": round(saturated_jobs / swall, 3),
+                          "p50_ms": round(float(np.percentile(slat, 50)), 1),
+                          "p99_ms": round(float(np.percentile(slat, 99)), 1),
+                          "max_active": int(sstats["max_active_seen"])},
+            "plain_percall_recons_per_s": round(plain, 3), "plain_sample_jobs": len(sample),
+            "speedup_vs_plain": round(served / plain, 2),
+            "saturated_speedup_vs_plain": round(saturated_jobs / swall / plain, 2)}
 
 
 def measure_fp32_peak(torch):
@@ -477,6 +557,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-subsets", type=int, default=1)
     ap.add_argument("--no-extras", action="store_true", help="skip the batched/served measurements")
+    ap.add_argument("--served-jobs", type=int, default=500)
+    ap.add_argument("--served-rate", type=float, default=16.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

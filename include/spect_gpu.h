@@ -169,6 +169,36 @@ int spect_batch_set_job(spect_batch_t batch, int job, float* out, const float* x
 int spect_batch_run(spect_batch_t batch, void* stream);
 int spect_batch_destroy(spect_batch_t batch);
 
+/* Serving (no counterpart in the reference).  A server runs OS-EM
+ * reconstruction requests with continuous batching: a scheduler thread
+ * admits pending requests in arrival order while the device-memory budget
+ * (0 = half of the free memory) and max_active slots allow, keeps each
+ * admitted job's plan, PSF spectra, attenuation and iterate resident on the
+ * GPU, runs it on its own stream (jobs of different sizes overlap on the
+ * device), and frees its memory when it finishes so waiting requests can be
+ * admitted.  submit validates like SPECTplan/osem! (same messages), copies the
+ * host arrays and returns at once; wait blocks until the job is done (or
+ * timeout_ms, < 0 = forever), copies the reconstruction [nz][ny][nx] to `out`
+ * and the submit-to-finish latency to latency_ms.  stats: submitted, done,
+ * failed, active, pending, most active at once, bytes in use, budget. */
+typedef struct {
+  int nx, nz, px, pz, nview;     /* ny = nx */
+  const float* mumap;            /* [nz][ny][nx] */
+  const float* psfs;             /* [nview][ny][pz][px] */
+  float dy;
+  int interpmeth;                /* SPECT_INTERP_ONE / SPECT_INTERP_TWO */
+  const float* ynoisy;           /* [nview][nz][nx] */
+  const float* background;       /* [nview][nz][nx], > 0 */
+  const float* x0;               /* [nz][ny][nx] or NULL (ones) */
+  int nblocks, niter;
+} spect_job_desc;
+typedef struct spect_server_s* spect_server_t;
+int spect_server_create(spect_server_t* server, size_t device_budget, int max_active);
+int spect_server_submit(spect_server_t server, const spect_job_desc* job, long long* ticket);
+int spect_server_wait(spect_server_t server, long long ticket, float* out, double* latency_ms, int timeout_ms);
+int spect_server_stats(spect_server_t server, long long out[8]);
+int spect_server_destroy(spect_server_t server);
+
 /* Kernel accounting (no counterpart in the reference; measurement support).
  * spect_kernel_launches: number of kernels this library has launched in the
  * process.  spect_plan_profile(plan, on): when on, every kernel the plan

@@ -36,7 +36,7 @@ from . import _native
 from ._native import SpectError, check
 
 __all__ = [
-    "Batch", "SPECTplan", "project", "project_", "backproject", "backproject_", "mlem", "mlem_", "osem", "osem_",
+    "Batch", "Server", "SPECTplan", "project", "project_", "backproject", "backproject_", "mlem", "mlem_", "osem", "osem_",
     "Ablock", "psf_gauss", "nthreads", "SpectError",
 ]
 
@@ -347,6 +347,68 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             _native.lib().spect_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching reconstruction server (no counterpart in the reference).
+
+    ``Server(budget_bytes=0, max_active=16)``; ``submit(mumap, psfs, dy, ynoisy,
+    background, nblocks, niter, x0=None, interpmeth="two")`` returns a ticket at
+    once (host arrays in the reference's layout are copied); ``wait(ticket)``
+    returns ``(image, latency_ms)``.  Admission is by device-memory budget and
+    slots; admitted jobs keep their plan, spectra, attenuation and iterate on the
+    GPU and run concurrently on their own streams.
+    """
+
+    def __init__(self, budget_bytes=0, max_active=16):
+        h = ctypes.c_void_p()
+        check(_native.lib().spect_server_create(ctypes.byref(h), int(budget_bytes), int(max_active)))
+        self._h = h
+        self._shapes = {}
+
+    def submit(self, mumap, psfs, dy, ynoisy, background, nblocks, niter, x0=None, interpmeth="two"):
+        mu = np.asfortranarray(mumap, np.float32)
+        ps = np.asfortranarray(psfs, np.float32)
+        nx, ny, nz = mu.shape
+        px, pz, ny2, nview = ps.shape
+        if nx != ny:
+            raise SpectError(1, "nx != ny")
+        if ny2 != ny:
+            raise SpectError(8, "DimensionMismatch: image/psfs size")
+        y = _host_f32(ynoisy, (nx, nz, nview), "ynoisy")
+        b = _host_f32(background, (nx, nz, nview), "background")
+        x = None if x0 is None else _host_f32(x0, (nx, ny, nz), "x0")
+        d = _native.JobDesc(nx, nz, px, pz, nview, mu.ctypes.data, ps.ctypes.data, float(dy),
+                            {"one": 1, "two": 2}.get(interpmeth, interpmeth), y.ctypes.data, b.ctypes.data,
+                            None if x is None else x.ctypes.data, int(nblocks), int(niter))
+        t = ctypes.c_longlong()
+        check(_native.lib().spect_server_submit(self._h, ctypes.byref(d), ctypes.byref(t)))
+        self._shapes[t.value] = (nx, ny, nz)
+        return t.value
+
+    def wait(self, ticket, timeout_ms=-1):
+        shape = self._shapes.pop(ticket)
+        out = np.empty(shape, np.float32, order="F")
+        lat = ctypes.c_double()
+        check(_native.lib().spect_server_wait(self._h, ticket, _ptr(out), ctypes.byref(lat), int(timeout_ms)))
+        return out, lat.value
+
+    def stats(self):
+        v = (ctypes.c_longlong * 8)()
+        check(_native.lib().spect_server_stats(self._h, v))
+        keys = ("submitted", "done", "failed", "active", "pending", "max_active_seen", "bytes_in_use", "budget")
+        return dict(zip(keys, list(v)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _native.lib().spect_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -16,6 +16,16 @@ _I = ctypes.c_int
 _F = ctypes.c_float
 _Z = ctypes.c_size_t
 
+class JobDesc(ctypes.Structure):
+    """spect_job_desc of include/spect_gpu.h."""
+
+    _fields_ = [("nx", ctypes.c_int), ("nz", ctypes.c_int), ("px", ctypes.c_int), ("pz", ctypes.c_int),
+                ("nview", ctypes.c_int), ("mumap", ctypes.c_void_p), ("psfs", ctypes.c_void_p),
+                ("dy", ctypes.c_float), ("interpmeth", ctypes.c_int), ("ynoisy", ctypes.c_void_p),
+                ("background", ctypes.c_void_p), ("x0", ctypes.c_void_p), ("nblocks", ctypes.c_int),
+                ("niter", ctypes.c_int)]
+
+
 _SIGS = {
     "spect_last_error": ([], ctypes.c_char_p),
     "spect_device_info": ([ctypes.POINTER(_I), ctypes.POINTER(_Z)], _I),
@@ -37,6 +47,11 @@ _SIGS = {
     "spect_batch_set_job": ([_P, _I, _P, _P, _P, _P], _I),
     "spect_batch_run": ([_P, _P], _I),
     "spect_batch_destroy": ([_P], _I),
+    "spect_server_create": ([ctypes.POINTER(_P), _Z, _I], _I),
+    "spect_server_submit": ([_P, ctypes.POINTER(JobDesc), ctypes.POINTER(ctypes.c_longlong)], _I),
+    "spect_server_wait": ([_P, ctypes.c_longlong, _P, ctypes.POINTER(ctypes.c_double), _I], _I),
+    "spect_server_stats": ([_P, _P], _I),
+    "spect_server_destroy": ([_P], _I),
     "spect_kernel_launches": ([], ctypes.c_ulonglong),
     "spect_plan_profile": ([_P, _I], _I),
     "spect_plan_kernel_times": ([_P, _P, _P], _I),

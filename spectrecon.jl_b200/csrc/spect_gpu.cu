@@ -22,6 +22,11 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -201,6 +206,10 @@ struct spect_plan_s {
   int rota_smem_ok = 1, nsplit_adj = 1;
   size_t rota_smem = 0;
   size_t bytes = 0;
+  // stream on which the plan is built and its buffers are (de)allocated;
+  // async_alloc: cudaMallocAsync/cudaFreeAsync on it (no device-wide sync)
+  cudaStream_t home = 0;
+  bool async_alloc = false;
   Profiler prof;
   std::mutex mu;
 };
@@ -210,7 +219,7 @@ namespace {
 template <class T>
 int dalloc(spect_plan_s* p, T** ptr, size_t count) {
   size_t b = sizeof(T) * std::max<size_t>(count, 1);
-  cudaError_t e = cudaMalloc((void**)ptr, b);
+  cudaError_t e = p->async_alloc ? cudaMallocAsync((void**)ptr, b, p->home) : cudaMalloc((void**)ptr, b);
   if (e != cudaSuccess) {
     *ptr = nullptr;
     cudaGetLastError();
@@ -227,8 +236,25 @@ void free_plan(spect_plan_s* p) {
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
                   p->d_io_img, p->d_io_views};
   for (void* q : ptrs)
-    if (q) cudaFree(q);
+    if (q) {
+      if (p->async_alloc) cudaFreeAsync(q, p->home);
+      else cudaFree(q);
+    }
   delete p;
+}
+
+void dfree(spect_plan_s* p, void* q) {
+  if (!q) return;
+  if (p->async_alloc) cudaFreeAsync(q, p->home);
+  else cudaFree(q);
+}
+
+// host -> device copy of a host buffer that may go away after the call
+int upload(spect_plan_s* p, void* d, const void* h, size_t b) {
+  cudaError_t e = cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, p->home);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(p->home);
+  if (e != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+  return SPECT_OK;
 }
 
 int check_launch(const char* what) {
@@ -501,12 +527,12 @@ int ensure_em(spect_plan_s* p, int nblocks) {
   if (!p->d_ones) {
     STATUS_TRY(dalloc(p, &p->d_ones, V));
     std::vector<float> h(V, 1.0f);
-    CUDA_TRY(cudaMemcpy(p->d_ones, h.data(), sizeof(float) * V, cudaMemcpyHostToDevice));
+    STATUS_TRY(upload(p, p->d_ones, h.data(), sizeof(float) * V));
   }
   if (!p->d_flag) STATUS_TRY(dalloc(p, &p->d_flag, 1));
   if (p->asum_blocks < nblocks) {
     if (p->d_asum) {
-      cudaFree(p->d_asum);
+      dfree(p, p->d_asum);
       p->bytes -= sizeof(float) * p->N * p->asum_blocks;
     }
     p->d_asum = nullptr;
@@ -548,7 +574,7 @@ int prepare_osem(spect_plan_s* p, int nblocks, int niter) {
     std::vector<int> idx(p->nview);
     for (int b = 0; b < nblocks; ++b)
       for (int s = 0; s < nsub; ++s) idx[(size_t)b * nsub + s] = b + s * nblocks;
-    CUDA_TRY(cudaMemcpy(p->d_sub, idx.data(), sizeof(int) * p->nview, cudaMemcpyHostToDevice));
+    STATUS_TRY(upload(p, p->d_sub, idx.data(), sizeof(int) * p->nview));
     p->sub_nblocks = nblocks;
   }
   return SPECT_OK;
@@ -703,9 +729,19 @@ int spect_device_info(int* sm_count, size_t* total_mem) {
   return SPECT_OK;
 }
 
-int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview, const float* mumap,
-                      const float* psfs, float dy, const float* viewangle, int interpmeth, int mode, int nthread,
-                      int nthreads) {
+}  // extern "C"
+
+namespace {
+struct PlanOpts {
+  cudaStream_t home = 0;
+  bool async_alloc = false;
+  int gmax_cap = 0;     // > 0: at most this many views per group (scratch bound)
+  int atten_cache = -1; // -1 auto, 0 off (:two only), 1 on
+};
+
+int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview, const float* mumap,
+                     const float* psfs, float dy, const float* viewangle, int interpmeth, int mode, int nthread,
+                     int nthreads, const PlanOpts& opts) {
   if (!out || !mumap || !psfs) return fail(SPECT_ERR_ARG, "null pointer argument");
   *out = nullptr;
   if (nx <= 0 || ny <= 0 || nz <= 0 || px <= 0 || pz <= 0 || nview <= 0)
@@ -730,6 +766,8 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
                                            " exceeds this build's FFT limit of " + std::to_string(SPECT_TW_N));
 
   spect_plan_s* p = new spect_plan_s;
+  p->home = opts.home;
+  p->async_alloc = opts.async_alloc;
   p->nx = nx;
   p->ny = ny;
   p->nz = nz;
@@ -769,6 +807,7 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
       fr = 0;
     }
     bool want = !(env && env[0] == '0') && need <= std::min(fr / 4, (size_t)32 << 30);
+    if (opts.atten_cache >= 0) want = opts.atten_cache == 1;
     if (interpmeth == SPECT_INTERP_ONE) {
       // the :one path reads its attenuation from the cache
       int st1 = dalloc(p, &p->d_att, p->N * (size_t)nview);
@@ -813,6 +852,7 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
   // group size: rotated-plane scratch bounded by ~1 GiB
   const size_t budget = (size_t)1 << 30;
   p->gmax = (int)std::max<size_t>(1, std::min<size_t>((size_t)nview, budget / (sizeof(float) * p->N)));
+  if (opts.gmax_cap > 0) p->gmax = std::min(p->gmax, opts.gmax_cap);
 
   if ((st = dalloc(p, &p->d_mumap, p->N)) || (st = dalloc(p, &p->d_rot, nview)) ||
       (st = dalloc(p, &p->d_viewset, nview)) || (st = dalloc(p, &p->d_tw, SPECT_TW_N)) ||
@@ -831,11 +871,8 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
   }
   std::vector<int> all(nview);
   for (int v = 0; v < nview; ++v) all[v] = v;
-  auto up = [&](void* d, const void* h, size_t b) -> int {
-    cudaError_t e = cudaMemcpy(d, h, b, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
-    return SPECT_OK;
-  };
+  auto up = [&](void* d, const void* h, size_t b) -> int { return upload(p, d, h, b); };
+  const cudaStream_t hs = p->home;
   if ((st = up(p->d_mumap, mumap, sizeof(float) * p->N)) || (st = up(p->d_rot, rot.data(), sizeof(float4) * nview)) ||
       (st = up(p->d_viewset, p->view_set.data(), sizeof(int) * nview)) ||
       (st = up(p->d_tw, tw.data(), sizeof(float2) * SPECT_TW_N)) ||
@@ -895,14 +932,14 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
     for (int v0 = 0; v0 < nview && e == cudaSuccess; v0 += p->gmax) {
       const int nv = std::min(p->gmax, nview - v0);
       dim3 g1(nz, std::min(nv, p->r1_grid_y));
-      k_rot1_fwd<<<g1, kRot1Threads, p->r1f_smem_ok ? p->r1f_smem : 0>>>(
+      k_rot1_fwd<<<g1, kRot1Threads, p->r1f_smem_ok ? p->r1f_smem : 0, hs>>>(
           p->r1, p->d_mumap, 0, p->d_r1view, p->d_all + v0, nv, p->d_R1, p->r1f_smem_ok, p->d_gscr_r1);
       const size_t n = (size_t)nv * nz * nx;
-      k_att_scan<<<(int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16), 256>>>(
+      k_att_scan<<<(int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16), 256, 0, hs>>>(
           p->d_R1, nv, nx, ny, nz, dy, p->d_att + (size_t)v0 * p->N);
       e = cudaGetLastError();
     }
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(hs);
     if (e != cudaSuccess) {
       fail(SPECT_ERR_CUDA, std::string("attenuation cache (:one): ") + cudaGetErrorString(e));
       return bail(SPECT_ERR_CUDA);
@@ -911,11 +948,12 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
     dim3 grid(nz, std::max(1, std::min(cdiv(2 * p->sm_count, nz), cdiv(nview, p->rotf_vpb))));
     const int thr = nx * p->rotf_vpb;
     if (p->att_smem_ok)
-      k_atten_build<true><<<grid, thr, sizeof(float) * (size_t)nx * ny>>>(g, p->d_mumap, p->d_rot, nview, p->d_att);
+      k_atten_build<true><<<grid, thr, sizeof(float) * (size_t)nx * ny, hs>>>(g, p->d_mumap, p->d_rot, nview,
+                                                                                p->d_att);
     else
-      k_atten_build<false><<<grid, thr>>>(g, p->d_mumap, p->d_rot, nview, p->d_att);
+      k_atten_build<false><<<grid, thr, 0, hs>>>(g, p->d_mumap, p->d_rot, nview, p->d_att);
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(hs);
     if (e != cudaSuccess) {
       fail(SPECT_ERR_CUDA, std::string("attenuation cache: ") + cudaGetErrorString(e));
       return bail(SPECT_ERR_CUDA);
@@ -933,21 +971,24 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
     double2 *d_wx = nullptr, *d_wz = nullptr, *d_G = nullptr;
     float* d_psf = nullptr;
     float* d_Hfull = nullptr;
+    auto tmalloc = [&](void** q, size_t b) {
+      return p->async_alloc ? cudaMallocAsync(q, b, hs) : cudaMalloc(q, b);
+    };
     auto cleanup = [&]() {
-      if (d_wx) cudaFree(d_wx);
-      if (d_wz) cudaFree(d_wz);
-      if (d_G) cudaFree(d_G);
-      if (d_psf) cudaFree(d_psf);
-      if (d_Hfull) cudaFree(d_Hfull);
+      dfree(p, d_wx);
+      dfree(p, d_wz);
+      dfree(p, d_G);
+      dfree(p, d_psf);
+      dfree(p, d_Hfull);
     };
     cudaError_t e = cudaSuccess;
-    e = cudaMalloc((void**)&d_wx, sizeof(double2) * Npx);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&d_wz, sizeof(double2) * Npz);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&d_G, per_plane_G * batch);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&d_psf, sizeof(float) * pp * batch);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&d_Hfull, sizeof(float) * g.Hz * Npx * batch);
-    if (e == cudaSuccess) e = cudaMemcpy(d_wx, wx.data(), sizeof(double2) * Npx, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_wz, wz.data(), sizeof(double2) * Npz, cudaMemcpyHostToDevice);
+    e = tmalloc((void**)&d_wx, sizeof(double2) * Npx);
+    if (e == cudaSuccess) e = tmalloc((void**)&d_wz, sizeof(double2) * Npz);
+    if (e == cudaSuccess) e = tmalloc((void**)&d_G, per_plane_G * batch);
+    if (e == cudaSuccess) e = tmalloc((void**)&d_psf, sizeof(float) * pp * batch);
+    if (e == cudaSuccess) e = tmalloc((void**)&d_Hfull, sizeof(float) * g.Hz * Npx * batch);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_wx, wx.data(), sizeof(double2) * Npx, cudaMemcpyHostToDevice, hs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_wz, wz.data(), sizeof(double2) * Npz, cudaMemcpyHostToDevice, hs);
     std::vector<float> hp(pp * batch);
     for (size_t b0 = 0; e == cudaSuccess && b0 < nplanes; b0 += batch) {
       size_t nb = std::min(batch, nplanes - b0);
@@ -956,18 +997,18 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
         size_t set = pl / ny, y = pl % ny;
         std::memcpy(hp.data() + q * pp, psfs + ((size_t)uniq[set] * ny + y) * pp, sizeof(float) * pp);
       }
-      e = cudaMemcpy(d_psf, hp.data(), sizeof(float) * pp * nb, cudaMemcpyHostToDevice);
+      e = cudaMemcpyAsync(d_psf, hp.data(), sizeof(float) * pp * nb, cudaMemcpyHostToDevice, hs);
       if (e != cudaSuccess) break;
       int blocks = std::min(cdiv((long long)nb * pz * Npx, 256), p->sm_count * 32);
-      k_psf_stage1<<<blocks, 256>>>(d_psf, (int)nb, px, pz, Npx, d_wx, d_G);
+      k_psf_stage1<<<blocks, 256, 0, hs>>>(d_psf, (int)nb, px, pz, Npx, d_wx, d_G);
       blocks = std::min(cdiv((long long)nb * g.Hz * Npx, 256), p->sm_count * 32);
-      k_psf_stage2<<<blocks, 256>>>(d_G, (int)nb, pz, Npx, Npz, g.Hz, d_wz, d_Hfull);
+      k_psf_stage2<<<blocks, 256, 0, hs>>>(d_G, (int)nb, pz, Npx, Npz, g.Hz, d_wz, d_Hfull);
       const ConvGeom& cg = p->cg;
       blocks = std::min(cdiv((long long)nb * (cg.Q + 1) * Npx, 256), p->sm_count * 32);
-      k_psf_permute<<<blocks, 256>>>(d_Hfull, (int)nb, Npx, Npz, g.Hz, p->RX, cg.logCX, p->RZ, cg.logCZ, cg.Q,
+      k_psf_permute<<<blocks, 256, 0, hs>>>(d_Hfull, (int)nb, Npx, Npz, g.Hz, p->RX, cg.logCX, p->RZ, cg.logCZ, cg.Q,
                                      p->d_H + b0 * (cg.Q + 1) * Npx);
       e = cudaGetLastError();
-      if (e == cudaSuccess) e = cudaDeviceSynchronize();
+      if (e == cudaSuccess) e = cudaStreamSynchronize(hs);
     }
     cleanup();
     if (e != cudaSuccess) {
@@ -977,6 +1018,16 @@ int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz,
   }
   *out = p;
   return SPECT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int spect_plan_create(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview, const float* mumap,
+                      const float* psfs, float dy, const float* viewangle, int interpmeth, int mode, int nthread,
+                      int nthreads) {
+  return plan_create_impl(out, nx, ny, nz, px, pz, nview, mumap, psfs, dy, viewangle, interpmeth, mode, nthread,
+                          nthreads, PlanOpts());
 }
 
 int spect_plan_destroy(spect_plan_t p) {
@@ -1270,6 +1321,344 @@ int spect_psf_gauss(float* psf, int ny, int px, int pz, const double* fwhm_x, co
     for (int j = 0; j < pz; ++j)
       for (int i = 0; i < px; ++i) psf[((size_t)y * pz + j) * px + i] = (float)(wx[i] * wz[j]);
   }
+  return SPECT_OK;
+}
+
+}  // extern "C"
+
+// ======================================================================
+// Serving: continuous batching of OS-EM reconstruction requests.
+// A scheduler thread admits pending jobs (FIFO) while a device-memory budget
+// and a slot limit allow, builds each job's plan on the job's own
+// non-blocking stream with stream-ordered allocation (no device-wide
+// synchronisation, so admissions never stall running jobs), enqueues the
+// whole osem! on that stream, and polls completion events; finished jobs
+// release their memory and free slots for the next ones.  The jobs' work
+// overlaps on the GPU.
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServerJob {
+  long long ticket = 0;
+  int nx = 0, nz = 0, px = 0, pz = 0, nview = 0, interp = 2, nblocks = 1, niter = 1;
+  float dy = 1.f;
+  std::vector<float> mumap, psfs, y, bg, x0, result;
+  int state = 0;  // 0 pending, 1 active, 2 done, 3 failed
+  int status = SPECT_OK;
+  std::string err;
+  Clock::time_point t_submit, t_admit, t_done;
+  size_t est = 0, bytes = 0;
+  spect_plan_s* plan = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev = nullptr;
+  float *d_x = nullptr, *d_x0 = nullptr, *d_y = nullptr, *d_bg = nullptr;
+};
+
+size_t est_job_bytes(const ServerJob& j, bool att) {
+  const size_t N = (size_t)j.nx * j.nx * j.nz, nxz = (size_t)j.nx * j.nz;
+  const int Npx = power2(j.nx + j.px - 1), Npz = power2(j.nz + j.pz - 1);
+  const size_t Q = std::max(1, Npz / 2), nsub = j.nview / j.nblocks;
+  size_t f = N                                       // mumap
+             + (att ? (size_t)j.nview * N : 0)        // attenuation cache
+             + (size_t)j.nx * (Q + 1) * Npx           // PSF spectra (one set)
+             + nsub * N + nsub * 16 * nxz + 2 * nsub * Q * Npx  // P, part, Vs
+             + 8 * N + 2 * (size_t)j.nview * nxz + (size_t)j.nblocks * N  // imgpart, EM buffers
+             + 2 * N + 2 * (size_t)j.nview * nxz;     // job buffers
+  if (j.interp == SPECT_INTERP_ONE) f += nsub * N;
+  size_t b = 4 * f + (size_t)j.nview * 32;
+  // per-CTA global slabs of large planes (B, spectra accumulators)
+  if ((size_t)j.nx * (Q + 1) * 8 + 8192 > 227 * 1024) b += (size_t)148 * j.nx * (Q + 1) * 8;
+  if ((Npx / std::min(32, Npx)) * (Npz / std::min(32, Npz)) > 32) b += (size_t)148 * Q * Npx * 8;
+  return b + b / 10 + ((size_t)16 << 20);
+}
+
+}  // namespace
+
+struct spect_server_s {
+  size_t budget = 0;
+  int max_active = 1;
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<ServerJob*> pending;
+  std::vector<ServerJob*> active;
+  std::unordered_map<long long, ServerJob*> jobs;
+  long long next_ticket = 1;
+  size_t used = 0;
+  bool stop = false;
+  long long n_submitted = 0, n_done = 0, n_failed = 0, max_active_seen = 0;
+  float* staging = nullptr;  // pinned result staging
+  size_t staging_n = 0;
+  std::thread worker;
+};
+
+namespace {
+
+void job_release(ServerJob* j) {
+  if (j->plan) free_plan(j->plan);  // stream-ordered frees on the job's stream
+  j->plan = nullptr;
+  float* bufs[] = {j->d_x, j->d_x0, j->d_y, j->d_bg};
+  for (float* q : bufs)
+    if (q) cudaFreeAsync(q, j->st);
+  j->d_x = j->d_x0 = j->d_y = j->d_bg = nullptr;
+  if (j->ev) cudaEventDestroy(j->ev);
+  if (j->st) cudaStreamDestroy(j->st);  // released once its queued frees ran
+  j->ev = nullptr;
+  j->st = nullptr;
+  std::vector<float>().swap(j->mumap);
+  std::vector<float>().swap(j->psfs);
+  std::vector<float>().swap(j->y);
+  std::vector<float>().swap(j->bg);
+  std::vector<float>().swap(j->x0);
+}
+
+int job_admit(ServerJob* j, size_t budget) {
+  CUDA_TRY(cudaStreamCreateWithFlags(&j->st, cudaStreamNonBlocking));
+  CUDA_TRY(cudaEventCreateWithFlags(&j->ev, cudaEventDisableTiming));
+  PlanOpts o;
+  o.home = j->st;
+  o.async_alloc = true;
+  o.gmax_cap = j->nview / j->nblocks;
+  const size_t att = sizeof(float) * (size_t)j->nx * j->nx * j->nz * j->nview;
+  o.atten_cache = (j->interp == SPECT_INTERP_ONE || att <= budget / 8) ? 1 : 0;
+  spect_plan_t plan = nullptr;
+  STATUS_TRY(plan_create_impl(&plan, j->nx, j->nx, j->nz, j->px, j->pz, j->nview, j->mumap.data(), j->psfs.data(),
+                              j->dy, nullptr, j->interp, SPECT_MODE_FAST, 1, 1, o));
+  j->plan = plan;
+  const size_t N = plan->N, V = (size_t)j->nview * plan->nxz;
+  STATUS_TRY(dalloc(plan, &j->d_x, N));
+  STATUS_TRY(dalloc(plan, &j->d_x0, N));
+  STATUS_TRY(dalloc(plan, &j->d_y, V));
+  STATUS_TRY(dalloc(plan, &j->d_bg, V));
+  // the plan frees what dalloc took; keep job buffers out of its list
+  CUDA_TRY(cudaMemcpyAsync(j->d_x0, j->x0.data(), sizeof(float) * N, cudaMemcpyHostToDevice, j->st));
+  CUDA_TRY(cudaMemcpyAsync(j->d_y, j->y.data(), sizeof(float) * V, cudaMemcpyHostToDevice, j->st));
+  CUDA_TRY(cudaMemcpyAsync(j->d_bg, j->bg.data(), sizeof(float) * V, cudaMemcpyHostToDevice, j->st));
+  STATUS_TRY(prepare_osem(plan, j->nblocks, j->niter));
+  STATUS_TRY(enqueue_osem(plan, j->d_x, j->d_x0, j->d_y, j->d_bg, j->nblocks, j->niter, j->st));
+  CUDA_TRY(cudaEventRecord(j->ev, j->st));
+  j->bytes = std::max(plan->bytes, j->est);  // conservative accounting
+  return SPECT_OK;
+}
+
+void server_loop(spect_server_s* S) {
+  cudaSetDevice(S->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  for (;;) {
+    // completions
+    for (size_t i = 0; i < S->active.size();) {
+      ServerJob* j = S->active[i];
+      cudaError_t q = cudaEventQuery(j->ev);
+      if (q == cudaErrorNotReady) {
+        ++i;
+        continue;
+      }
+      const size_t N = j->plan ? j->plan->N : 0;
+      if (q == cudaSuccess) {
+        if (S->staging_n < N) {
+          if (S->staging) cudaFreeHost(S->staging);
+          S->staging = nullptr;
+          S->staging_n = 0;
+          if (cudaMallocHost((void**)&S->staging, sizeof(float) * N) == cudaSuccess) S->staging_n = N;
+        }
+        cudaError_t e = S->staging ? cudaMemcpyAsync(S->staging, j->d_x, sizeof(float) * N, cudaMemcpyDeviceToHost,
+                                                     j->st)
+                                   : cudaErrorMemoryAllocation;
+        if (e == cudaSuccess) e = cudaStreamSynchronize(j->st);
+        if (e == cudaSuccess) {
+          j->result.assign(S->staging, S->staging + N);
+          j->state = 2;
+          S->n_done++;
+        } else {
+          j->state = 3;
+          j->status = SPECT_ERR_CUDA;
+          j->err = std::string("result copy: ") + cudaGetErrorString(e);
+          S->n_failed++;
+        }
+      } else {
+        j->state = 3;
+        j->status = SPECT_ERR_CUDA;
+        j->err = std::string("job execution: ") + cudaGetErrorString(q);
+        S->n_failed++;
+      }
+      j->t_done = Clock::now();
+      S->used -= std::min(S->used, j->bytes);
+      job_release(j);
+      S->active.erase(S->active.begin() + i);
+      S->cv_done.notify_all();
+    }
+    // admissions (FIFO) while slots and memory allow
+    while (!S->pending.empty() && (int)S->active.size() < S->max_active && !S->stop) {
+      ServerJob* j = S->pending.front();
+      if (j->est > S->budget) {
+        S->pending.pop_front();
+        j->state = 3;
+        j->status = SPECT_ERR_OOM;
+        j->err = "job needs about " + std::to_string(j->est) + " bytes, above the server budget of " +
+                 std::to_string(S->budget);
+        j->t_done = Clock::now();
+        S->n_failed++;
+        S->cv_done.notify_all();
+        continue;
+      }
+      if (S->used + j->est > S->budget) break;  // wait for memory to free up
+      S->pending.pop_front();
+      S->used += j->est;
+      lk.unlock();
+      j->t_admit = Clock::now();
+      int rc = job_admit(j, S->budget);
+      lk.lock();
+      S->used -= j->est;
+      if (rc != SPECT_OK) {
+        j->state = 3;
+        j->status = rc;
+        j->err = g_err;
+        j->t_done = Clock::now();
+        job_release(j);
+        S->n_failed++;
+        S->cv_done.notify_all();
+        continue;
+      }
+      S->used += j->bytes;
+      j->state = 1;
+      S->active.push_back(j);
+      S->max_active_seen = std::max<long long>(S->max_active_seen, (long long)S->active.size());
+    }
+    if (S->stop && S->active.empty()) break;
+    if (S->active.empty()) {
+      S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+    } else {
+      lk.unlock();
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+      lk.lock();
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int spect_server_create(spect_server_t* out, size_t device_budget, int max_active) {
+  if (!out || max_active < 1) return fail(SPECT_ERR_ARG, "bad spect_server_create arguments");
+  *out = nullptr;
+  spect_server_s* S = new spect_server_s;
+  if (cudaGetDevice(&S->device) != cudaSuccess) {
+    delete S;
+    return fail(SPECT_ERR_CUDA, "no CUDA device");
+  }
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
+  S->budget = device_budget ? device_budget : fr / 2;
+  S->max_active = max_active;
+  S->worker = std::thread(server_loop, S);
+  *out = S;
+  return SPECT_OK;
+}
+
+int spect_server_submit(spect_server_t S, const spect_job_desc* d, long long* ticket) {
+  if (!S || !d || !ticket || !d->mumap || !d->psfs || !d->ynoisy || !d->background)
+    return fail(SPECT_ERR_ARG, "bad spect_server_submit arguments");
+  if (d->nx <= 0 || d->nz <= 0 || d->px <= 0 || d->pz <= 0 || d->nview <= 0)
+    return fail(SPECT_ERR_ARG, "sizes must be positive");
+  if ((d->nx % 2)) return fail(SPECT_ERR_NX_ODD, "nx odd");
+  if (!(d->px % 2) || !(d->pz % 2)) return fail(SPECT_ERR_PSF_NOT_ODD, "non-odd size psfs");
+  if (d->interpmeth != SPECT_INTERP_ONE && d->interpmeth != SPECT_INTERP_TWO)
+    return fail(SPECT_ERR_INTERP, "bad interpmeth");
+  if (d->nblocks < 1 || d->nview % d->nblocks != 0) return fail(SPECT_ERR_NBLOCKS, "nview must be divisible by nblocks!");
+  if (d->niter < 0) return fail(SPECT_ERR_ARG, "niter must be >= 0");
+  const size_t N = (size_t)d->nx * d->nx * d->nz, V = (size_t)d->nx * d->nz * d->nview;
+  const size_t P = (size_t)d->px * d->pz * d->nx * d->nview;
+  for (size_t k = 0; k < V; ++k)
+    if (!(d->background[k] > 0.f)) return fail(SPECT_ERR_BACKGROUND, "need background > 0");
+  const size_t pp = (size_t)d->px * d->pz;
+  for (size_t pl = 0; pl < P / pp; ++pl)
+    for (size_t i = 0; i < pp; ++i)
+      if (!(d->psfs[pl * pp + i] == d->psfs[pl * pp + pp - 1 - i])) return fail(SPECT_ERR_PSF_ASYM, "asym. psf");
+  if (power2(d->nx + d->px - 1) > SPECT_TW_N || power2(d->nz + d->pz - 1) > SPECT_TW_N)
+    return fail(SPECT_ERR_UNSUPPORTED, "padded plane exceeds this build's FFT limit");
+  ServerJob* j = new ServerJob;
+  j->nx = d->nx;
+  j->nz = d->nz;
+  j->px = d->px;
+  j->pz = d->pz;
+  j->nview = d->nview;
+  j->interp = d->interpmeth;
+  j->nblocks = d->nblocks;
+  j->niter = d->niter;
+  j->dy = d->dy;
+  j->mumap.assign(d->mumap, d->mumap + N);
+  j->psfs.assign(d->psfs, d->psfs + P);
+  j->y.assign(d->ynoisy, d->ynoisy + V);
+  j->bg.assign(d->background, d->background + V);
+  if (d->x0) j->x0.assign(d->x0, d->x0 + N);
+  else j->x0.assign(N, 1.0f);
+  j->est = est_job_bytes(*j, j->interp == SPECT_INTERP_ONE ||
+                                 sizeof(float) * N * j->nview <= S->budget / 8);
+  j->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) {
+      delete j;
+      return fail(SPECT_ERR_BUSY, "server is shutting down");
+    }
+    j->ticket = S->next_ticket++;
+    S->jobs[j->ticket] = j;
+    S->pending.push_back(j);
+    S->n_submitted++;
+  }
+  S->cv_work.notify_one();
+  *ticket = j->ticket;
+  return SPECT_OK;
+}
+
+int spect_server_wait(spect_server_t S, long long ticket, float* out, double* latency_ms, int timeout_ms) {
+  if (!S) return fail(SPECT_ERR_ARG, "null server");
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->jobs.find(ticket);
+  if (it == S->jobs.end()) return fail(SPECT_ERR_ARG, "unknown ticket " + std::to_string(ticket));
+  ServerJob* j = it->second;
+  auto done = [&] { return j->state >= 2; };
+  if (timeout_ms < 0) S->cv_done.wait(lk, done);
+  else if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), done))
+    return fail(SPECT_ERR_TIMEOUT, "job " + std::to_string(ticket) + " not finished");
+  S->jobs.erase(it);
+  lk.unlock();
+  if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
+  int rc = j->status;
+  if (rc == SPECT_OK && out) std::memcpy(out, j->result.data(), sizeof(float) * j->result.size());
+  if (rc != SPECT_OK) g_err = j->err;
+  delete j;
+  return rc;
+}
+
+int spect_server_stats(spect_server_t S, long long out[8]) {
+  if (!S || !out) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  long long v[8] = {S->n_submitted, S->n_done, S->n_failed, (long long)S->active.size(),
+                    (long long)S->pending.size(), S->max_active_seen, (long long)S->used, (long long)S->budget};
+  std::memcpy(out, v, sizeof(v));
+  return SPECT_OK;
+}
+
+int spect_server_destroy(spect_server_t S) {
+  if (!S) return fail(SPECT_ERR_ARG, "null server");
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+    for (ServerJob* j : S->pending) {
+      j->state = 3;
+      j->status = SPECT_ERR_BUSY;
+      j->err = "server shut down before the job was admitted";
+    }
+    S->pending.clear();
+  }
+  S->cv_work.notify_all();
+  if (S->worker.joinable()) S->worker.join();  // running jobs finish first
+  for (auto& kv : S->jobs) delete kv.second;
+  if (S->staging) cudaFreeHost(S->staging);
+  delete S;
   return SPECT_OK;
 }
 
