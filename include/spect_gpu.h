@@ -106,7 +106,7 @@ int spect_project_host(spect_plan_t plan, float* views, const float* image, cons
  * views) lives in one file-scope device array of 32 MiB that every GPU
  * loading this library holds until the process exits; the views are
  * processed in groups that fit it, and a plan whose single view needs more
- * (nx*ny*nz + 16*nx*nz floats > 32 MiB) is rejected with
+ * (nx*ny*nz + 32*nx*nz floats > 32 MiB) is rejected with
  * SPECT_ERR_UNSUPPORTED.  The first call on a device looks up the array's
  * device address (cudaGetSymbolAddress); make that first call before any
  * stream capture.  All calls share the array and no part of it needs to
@@ -150,6 +150,15 @@ int spect_em_subset_update(spect_plan_t plan, float* x, const float* ynoisy, con
 /* asum = A_s' 1 with zeros replaced by +Inf (src/ml-os-em.jl:111-114). */
 int spect_subset_sensitivity(spect_plan_t plan, float* asum, const int32_t* index, int nindex,
                              void* stream);
+
+/* Autotuner (no counterpart in the reference).  Times candidate launch
+ * shapes of the plan's forward and adjoint projector for nindex views on the
+ * device (the depth-chunk tile of the FFT-convolution kernels, the view split
+ * of the rotation kernels) and keeps the fastest for calls with nindex views;
+ * results are cached per plan shape in the process.  ms[0], ms[1]: best
+ * forward and adjoint times.  Synchronous; spect_batch_create runs it for
+ * every job's subset size. */
+int spect_plan_autotune(spect_plan_t plan, int nindex, double ms[2]);
 
 /* Batched OS-EM (no counterpart in the reference: its osem! runs one
  * reconstruction at a time).  A batch holds njobs plans of any sizes (each

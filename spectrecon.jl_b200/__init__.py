@@ -148,6 +148,13 @@ class SPECTplan:
         d["device_bytes"] = b.value
         return d
 
+    def autotune(self, nindex=None):
+        """Time candidate launch shapes for calls with nindex views (default
+        nview) and keep the fastest; returns (forward_ms, adjoint_ms)."""
+        ms = (ctypes.c_double * 2)()
+        check(_native.lib().spect_plan_autotune(self._h, int(nindex or self.nview), ms))
+        return ms[0], ms[1]
+
     def close(self):
         if getattr(self, "_h", None):
             _native.lib().spect_plan_destroy(self._h)

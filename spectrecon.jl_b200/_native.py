@@ -43,6 +43,7 @@ _SIGS = {
     "spect_osem_host": ([_P, _P, _P, _P, _P, _I, _I], _I),
     "spect_em_subset_update": ([_P, _P, _P, _P, _P, _P, _I, _P], _I),
     "spect_subset_sensitivity": ([_P, _P, _P, _I, _P], _I),
+    "spect_plan_autotune": ([_P, _I, _P], _I),
     "spect_batch_create": ([ctypes.POINTER(_P), _I, _P, _P, _P], _I),
     "spect_batch_set_job": ([_P, _I, _P, _P, _P, _P], _I),
     "spect_batch_run": ([_P, _P], _I),

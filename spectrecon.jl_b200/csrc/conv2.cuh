@@ -28,6 +28,7 @@
 #include <stdint.h>
 
 #include "fft_reg.cuh"
+#include "bulk_copy.cuh"
 
 namespace spect {
 
@@ -60,6 +61,9 @@ struct Conv2Args {
   float2* gacc;         // per-CTA spectra slabs (Q*Npx) when they are not in registers
   const float2* tw;     // twiddles exp(-2 pi i m / SPECT_TW_N)
   int bsmem;
+  const float* att;     // attenuation cache [view][y][z][x]; att_mul: applied on plane load (forward)
+  int att_mul;
+  int* err;             // set to 1 when a bounded wait gives up
 };
 
 struct Lanes {
@@ -95,14 +99,15 @@ struct PlaneWalk {
   }
 };
 
-// real nz x nx plane (x fastest) -> real rows of B
+// real nz x nx plane (x fastest) -> real rows of B, times the attenuation
+// plane `att` when given
 __device__ __forceinline__ void load_plane(const ConvGeom& g, const PlaneWalk& W, float2* B,
-                                           const float* __restrict__ src) {
+                                           const float* __restrict__ src, const float* __restrict__ att) {
   float* Bf = reinterpret_cast<float*>(B);
   const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
   int x = W.x0, z = W.z0;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    Bf[x * rs + z] = __ldg(src + k);
+    Bf[x * rs + z] = att ? __fmul_rn(__ldg(src + k), __ldg(att + k)) : __ldg(src + k);
     x += W.dx;
     z += W.dz;
     if (x >= nx) {
@@ -112,14 +117,33 @@ __device__ __forceinline__ void load_plane(const ConvGeom& g, const PlaneWalk& W
   }
 }
 
-// real rows of B -> nz x nx plane (x fastest) in global memory
-__device__ __forceinline__ void store_plane(const ConvGeom& g, const PlaneWalk& W, const float2* B,
-                                            float* __restrict__ dst) {
+// real rows of B -> nz x nx plane (x fastest) in global memory, times the
+// attenuation plane staged in shared memory
+__device__ __forceinline__ void store_plane_satt(const ConvGeom& g, const PlaneWalk& W, const float2* B,
+                                                 float* __restrict__ dst, const float* satt) {
   const float* Bf = reinterpret_cast<const float*>(B);
   const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
   int x = W.x0, z = W.z0;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    dst[k] = Bf[x * rs + z];
+    dst[k] = __fmul_rn(satt[k], Bf[x * rs + z]);
+    x += W.dx;
+    z += W.dz;
+    if (x >= nx) {
+      x -= nx;
+      ++z;
+    }
+  }
+}
+
+// real rows of B -> nz x nx plane (x fastest) in global memory, times the
+// attenuation plane `att` when given
+__device__ __forceinline__ void store_plane(const ConvGeom& g, const PlaneWalk& W, const float2* B,
+                                            float* __restrict__ dst, const float* __restrict__ att) {
+  const float* Bf = reinterpret_cast<const float*>(B);
+  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
+  int x = W.x0, z = W.z0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    dst[k] = att ? __fmul_rn(__ldg(att + k), Bf[x * rs + z]) : Bf[x * rs + z];
     x += W.dx;
     z += W.dz;
     if (x >= nx) {
@@ -371,11 +395,31 @@ __device__ __forceinline__ void apply_psf(float2 (&v)[RX], const float* __restri
 
 // ------------------------------------------------------------------------
 // forward: persistent over items (slot, depth chunk)
-template <int RX, int RZ, bool REGACC>
+template <int RX, int RZ, bool REGACC, bool STAGE>
 __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
   const ConvGeom& g = a.g;
   FftTables TT;
   float2* B = conv_setup<RX, RZ>(a, &TT);
+  // STAGE: the next plane (and its attenuation) is bulk-copied into shared
+  // staging buffers while the current one is transformed
+  const int nplane = g.nz * g.nx;
+  float* sP = reinterpret_cast<float*>(B + (size_t)g.nx * g.QS);
+  float* sA = sP + nplane;
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sA + (a.att_mul ? nplane : 0));
+  unsigned phase = 0;
+  auto issue = [&](int item, int y) {
+    const int sl = item / a.nchunks;
+    const float* src = a.P + ((size_t)sl * g.ny + y) * nplane;
+    const float* asrc = a.att_mul ? a.att + ((size_t)a.vidx[sl] * g.ny + y) * nplane : nullptr;
+    tma_planes(bar, sP, src, sA, asrc, (unsigned)(nplane * sizeof(float)));
+  };
+  if (STAGE) {
+    if (threadIdx.x == 0) {
+      mbar_init(bar);
+      if ((int)blockIdx.x < a.nv * a.nchunks) issue(blockIdx.x, ((int)blockIdx.x % a.nchunks) * a.chunkY);
+    }
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Lanes L = lanes_of(lane, g.logCX);
   const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
@@ -393,9 +437,42 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
     const float* Pv = a.P + (size_t)slot * g.ny * g.nz * g.nx;
     const float* Hv = a.Hs + (size_t)a.viewset[a.vidx[slot]] * g.ny * (Q + 1) * Npx;
     for (int y = y0; y < y1; ++y) {
-      __syncthreads();
-      load_plane(g, W, B, Pv + (size_t)y * g.nz * g.nx);
-      __syncthreads();
+      if (STAGE) {
+        // the block barrier also frees B from the previous plane
+        if (__syncthreads_or(!mbar_wait(bar, phase))) {
+          // a copy that never completed: flag it, give it one more bounded
+          // wait, and leave the block
+          if (threadIdx.x == 0) {
+            atomicExch(a.err, 1);
+            mbar_wait(bar, phase);
+          }
+          return;
+        }
+        phase ^= 1u;
+        float* Bf = reinterpret_cast<float*>(B);
+        const int rs = 2 * g.QS;
+        int x = W.x0, z = W.z0;
+        for (int k = threadIdx.x; k < nplane; k += blockDim.x) {
+          Bf[x * rs + z] = a.att_mul ? __fmul_rn(sP[k], sA[k]) : sP[k];
+          x += W.dx;
+          z += W.dz;
+          if (x >= g.nx) {
+            x -= g.nx;
+            ++z;
+          }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {  // prefetch the next plane of this CTA
+          if (y + 1 < y1) issue(item, y + 1);
+          else if (item + (int)gridDim.x < nitems)
+            issue(item + gridDim.x, ((item + (int)gridDim.x) % a.nchunks) * a.chunkY);
+        }
+      } else {
+        __syncthreads();
+        load_plane(g, W, B, Pv + (size_t)y * g.nz * g.nx,
+                   a.att_mul ? a.att + ((size_t)a.vidx[slot] * g.ny + y) * g.nz * g.nx : nullptr);
+        __syncthreads();
+      }
       zfft_rows_fwd<RZ, false>(g, B, TT, warp, lane, T.zrd);
       __syncthreads();
       const float* Hy = Hv + (size_t)y * (Q + 1) * Npx;
@@ -408,9 +485,16 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
           float2 v[RX];
 #pragma unroll
           for (int r = 0; r < RX; ++r) v[r] = B[T.xrd[r] + cc];
+          float hp[RX];  // PSF spectrum loads issued before the transform
+#pragma unroll
+          for (int k1 = 0; k1 < RX; ++k1) hp[k1] = __ldg(Hy + (size_t)cc * Npx + L.l + k1 * CX);
           fft_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
-          apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX,
-                        j == 0 && warp == 0, cc == 0);
+          if (j == 0 && warp == 0) {
+            apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX, true, cc == 0);
+          } else {
+#pragma unroll
+            for (int k1 = 0; k1 < RX; ++k1) v[k1] = cscale(v[k1], hp[k1]);
+          }
           if (active) {
             if (REGACC) {
 #pragma unroll
@@ -453,7 +537,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
     __syncthreads();
     zfft_rows_inv<RZ, false>(g, B, TT, warp, lane, TW.zg);
     __syncthreads();
-    store_plane(g, W, B, a.part + ((size_t)slot * a.nchunks + ch) * g.nz * g.nx);
+    store_plane(g, W, B, a.part + ((size_t)slot * a.nchunks + ch) * g.nz * g.nx, nullptr);
   }
 }
 
@@ -473,7 +557,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
   T.init(g, lane, true);
   for (int slot = blockIdx.x; slot < a.nv; slot += gridDim.x) {
     __syncthreads();
-    load_plane(g, W, B, a.views + (size_t)slot * g.nz * g.nx);
+    load_plane(g, W, B, a.views + (size_t)slot * g.nz * g.nx, nullptr);
     __syncthreads();
     zfft_rows_fwd<RZ, true>(g, B, TT, warp, lane, T.zrd);
     __syncthreads();
@@ -495,11 +579,24 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
 
 // ------------------------------------------------------------------------
 // adjoint: persistent over items (slot, depth chunk); T[slot][y][z][x]
-template <int RX, int RZ, bool REGACC>
+template <int RX, int RZ, bool REGACC, bool STAGE>
 __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
   const ConvGeom& g = a.g;
   FftTables TT;
   float2* B = conv_setup<RX, RZ>(a, &TT);
+  // STAGE: the attenuation plane of each output plane is bulk-copied into
+  // shared memory while the plane is transformed, and multiplied in on store.
+  // Shared memory: [FFT tables][B when bsmem][attenuation plane][mbarrier]
+  const int nplane = g.nz * g.nx;
+  extern __shared__ float4 smem4[];
+  float* sA = reinterpret_cast<float*>(reinterpret_cast<char*>(smem4) + fft_tables_bytes(RX, RZ) +
+                                       (a.bsmem ? sizeof(float2) * (size_t)g.nx * g.QS : 0));
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sA + nplane);
+  unsigned phase = 0;
+  if (STAGE) {
+    if (threadIdx.x == 0) mbar_init(bar);
+    __syncthreads();
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const Lanes L = lanes_of(lane, g.logCX);
   const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
@@ -528,6 +625,11 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
     for (int y = y0; y < y1; ++y) {
       const float* Hy = Hv + (size_t)y * (Q + 1) * Npx;
       __syncthreads();
+      if (STAGE && threadIdx.x == 0) {
+        fence_proxy_async();
+        mbar_expect(bar, (unsigned)(nplane * sizeof(float)));
+        bulk_copy(bar, sA, a.att + ((size_t)a.vidx[slot] * g.ny + y) * nplane, (unsigned)(nplane * sizeof(float)));
+      }
 #pragma unroll
       for (int j = 0; j < JM; ++j) {
         if (j < JC) {
@@ -567,8 +669,20 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
       }
       __syncthreads();
       zfft_rows_inv<RZ, true>(g, B, TT, warp, lane, T.zg);
-      __syncthreads();
-      store_plane(g, W, B, a.T + ((size_t)slot * g.ny + y) * g.nz * g.nx);
+      if (STAGE) {
+        if (__syncthreads_or(!mbar_wait(bar, phase))) {
+          if (threadIdx.x == 0) {
+            atomicExch(a.err, 1);
+            mbar_wait(bar, phase);
+          }
+          return;
+        }
+        phase ^= 1u;
+        store_plane_satt(g, W, B, a.T + ((size_t)slot * g.ny + y) * g.nz * g.nx, sA);
+      } else {
+        __syncthreads();
+        store_plane(g, W, B, a.T + ((size_t)slot * g.ny + y) * g.nz * g.nx, nullptr);
+      }
     }
   }
 }

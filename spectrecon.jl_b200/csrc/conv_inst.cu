@@ -13,11 +13,15 @@
 namespace spect {
 
 namespace {
+// kind 0 forward, 1 adjoint, 2 view spectra, 3 forward with plane staging,
+// 4 adjoint with staged attenuation multiplied on store
 template <int RZ>
 const void* kernel_ptr(int kind) {
   constexpr bool REG = SPECT_RX * RZ <= 32;
-  if (kind == 0) return (const void*)k_conv_fwd2<SPECT_RX, RZ, REG>;
-  if (kind == 1) return (const void*)k_conv_adj2<SPECT_RX, RZ, REG>;
+  if (kind == 0) return (const void*)k_conv_fwd2<SPECT_RX, RZ, REG, false>;
+  if (kind == 3) return (const void*)k_conv_fwd2<SPECT_RX, RZ, REG, true>;
+  if (kind == 1) return (const void*)k_conv_adj2<SPECT_RX, RZ, REG, false>;
+  if (kind == 4) return (const void*)k_conv_adj2<SPECT_RX, RZ, REG, true>;
   return (const void*)k_vspec2<SPECT_RX, RZ>;
 }
 const void* kernel_ptr_rt(int kind, int RZ) {
@@ -32,7 +36,6 @@ const void* kernel_ptr_rt(int kind, int RZ) {
 }
 }  // namespace
 
-// kind 0 forward, 1 adjoint, 2 view spectra
 cudaError_t SPECT_CAT(conv2_launch_rx, SPECT_RX)(int kind, int RZ, int grid, size_t smem, cudaStream_t st,
                                                  const Conv2Args& a) {
   const void* k = kernel_ptr_rt(kind, RZ);
@@ -49,7 +52,7 @@ cudaError_t SPECT_CAT(conv2_setup_rx, SPECT_RX)(int RZ, size_t smem, int* occ) {
   cudaError_t e0 = cudaGetDevice(&dev);
   if (e0 == cudaSuccess) e0 = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e0 != cudaSuccess) return e0;
-  for (int kind = 0; kind < 3; ++kind) {
+  for (int kind = 0; kind < 5; ++kind) {
     const void* k = kernel_ptr_rt(kind, RZ);
     if (!k) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);

@@ -176,7 +176,7 @@ struct spect_plan_s {
   int* d_all = nullptr;  // 0..nview-1
   int* d_idx = nullptr;  // per-call index staging [nview]
   // work scratch for one group of views
-  int gmax = 1, nchunk_max = 16;
+  int gmax = 1, nchunk_max = 32;
   float* d_P = nullptr;
   float* d_part = nullptr;
   float2* d_Vs = nullptr;
@@ -200,10 +200,19 @@ struct spect_plan_s {
   int RX = 1, RZ = 1;
   int conv_grid = 148, conv_bsmem = 1;
   size_t conv_smem = 0;
+  int conv_stage = 0;         // forward kernel stages planes by bulk copy
+  size_t conv_smem_fwd = 0;   // its shared memory
+  int adj_stage = 0;          // adjoint convolution multiplies the staged attenuation on store and
+                              // the adjoint rotation bulk-copies its (premultiplied) slices
+  size_t conv_smem_adj = 0, rota_smem_stage = 0;
+  int rot_nband = 0;          // bands of output rows (adj_stage 2)
+  int* d_err = nullptr;       // bounded-wait give-ups
   int rotf_vpb = 1, rotf_smem_ok = 1;
   size_t rotf_smem = 0;
   int att_smem_ok = 1;
-  int rota_smem_ok = 1, nsplit_adj = 1;
+  int rota_smem_ok = 1, nsplit_adj = 1, nsplit_adj_max = 1;
+  // tuned launch shapes (0 = analytic default); tuned_nv = the view count they were tuned for
+  int tune_fwd_cy = 0, tune_adj_cy = 0, tune_rotf_nsplit = 0, tuned_nv = 0;
   size_t rota_smem = 0;
   size_t bytes = 0;
   // stream on which the plan is built and its buffers are (de)allocated;
@@ -231,7 +240,7 @@ int dalloc(spect_plan_s* p, T** ptr, size_t count) {
 }
 
 void free_plan(spect_plan_s* p) {
-  void* ptrs[] = {p->d_mumap, p->d_att, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
+  void* ptrs[] = {p->d_mumap, p->d_att, p->d_err, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
                   p->d_io_img, p->d_io_views};
@@ -327,6 +336,17 @@ int configure(spect_plan_s* p) {
   }
   if (ce != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string("conv kernel setup: ") + cudaGetErrorString(ce));
   p->conv_grid = p->sm_count * std::max(occ, 1);
+  // plane staging of the forward kernel: B in shared memory, planes of a
+  // multiple of 16 bytes, room for the staging buffers (+ attenuation)
+  {
+    const size_t nplane = (size_t)g.nx * g.nz;
+    const size_t stage = sizeof(float) * nplane * 2 + 16;
+    p->conv_stage = (p->conv_bsmem && (nplane % 4) == 0 && p->conv_smem + stage <= p->max_smem &&
+                     !(std::getenv("SPECT_NO_STAGE") && std::getenv("SPECT_NO_STAGE")[0] == '1'))
+                        ? 1
+                        : 0;
+    p->conv_smem_fwd = p->conv_smem + (p->conv_stage ? stage : 0);
+  }
   if (!p->conv_bsmem) STATUS_TRY(dalloc(p, &p->d_gB, (size_t)g.nx * cg.QS * p->conv_grid));
   if (p->RX * p->RZ > 32) STATUS_TRY(dalloc(p, &p->d_gacc, (size_t)cg.Q * g.Npx * p->conv_grid));
   // ---- forward rotation
@@ -349,21 +369,79 @@ int configure(spect_plan_s* p) {
   p->rota_smem = (2 * slice + (size_t)nseg * g.nx) * sizeof(float);
   p->rota_smem_ok = p->rota_smem <= p->max_smem;
   p->nsplit_adj = std::max(1, std::min(8, cdiv(2 * p->sm_count, g.nz)));
+  // the autotuner may try up to 16 view splits when the split partial images stay small
+  p->nsplit_adj_max = (sizeof(float) * p->N * 16 <= ((size_t)256 << 20) && p->rota_smem <= p->max_smem)
+                          ? std::max(p->nsplit_adj, 16)
+                          : p->nsplit_adj;
   if (p->rota_smem_ok) {
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
   } else {
     size_t per = 2 * slice + (size_t)nseg * g.nx;
-    STATUS_TRY(dalloc(p, &p->d_gscr_adj, per * g.nz * p->nsplit_adj));
+    STATUS_TRY(dalloc(p, &p->d_gscr_adj, per * g.nz * p->nsplit_adj_max));
+  }
+  // staged adjoint (attenuation cache, :two): the adjoint convolution
+  // multiplies the bulk-copied attenuation plane into its output on store, and
+  // the adjoint rotation bulk-copies those premultiplied slices into two
+  // shared buffers (rows of nx floats: nx a multiple of 4 for 16-byte copies)
+  {
+    const size_t nplane = (size_t)g.nx * g.nz;
+    const size_t cadj = p->conv_smem + sizeof(float) * nplane + 16;
+    const char* ns = std::getenv("SPECT_NO_STAGE");
+    const bool ok = p->d_att && p->interp == SPECT_INTERP_TWO && (g.nx % 4) == 0 && cadj <= p->max_smem &&
+                    !(ns && ns[0] == '1');
+    // 1: whole slices (accumulator + two slices); 2: bands of output rows
+    // (accumulator band + two chunks of kRotBandRows rows)
+    const size_t rsm = 3 * slice * sizeof(float) + 16;
+    int nband = 0;
+    size_t bsm = 0;
+    for (int nb = 2; nb <= g.ny && ok && rsm > p->max_smem; ++nb) {
+      bsm = sizeof(float) * ((size_t)cdiv(g.ny, nb) * g.nx + 2 * (size_t)kRotBandRows * g.nx) + 16;
+      if (bsm <= p->max_smem) {
+        nband = nb;
+        break;
+      }
+    }
+    p->adj_stage = !ok ? 0 : rsm <= p->max_smem ? 1 : nband ? 2 : 0;
+    p->rot_nband = nband;
+    p->conv_smem_adj = p->adj_stage ? cadj : p->conv_smem;
+    p->rota_smem_stage = p->adj_stage == 1 ? rsm : bsm;
+    if (p->adj_stage == 1)
+      CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)p->max_smem));
+    if (p->adj_stage == 2)
+      CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj_band, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)p->max_smem));
   }
   return SPECT_OK;
 }
 
 // chunking of the depth planes for a call with nv views
-void chunking(const spect_plan_s* p, int nv, int* chunkY, int* nchunks) {
-  int target = 4 * p->conv_grid;
-  int nc = std::max(1, std::min(std::min(p->nchunk_max, p->ny), cdiv(target, std::max(nv, 1))));
-  int cy = cdiv(p->ny, nc);
+// depth-chunk tile of the persistent convolution kernels: items = nv x
+// ceil(ny/cy) are dealt round-robin to conv_grid CTAs, so the makespan is
+// ceil(items/grid) x (cy + c0) plane costs (c0: per-item overhead, the
+// chunk's inverse transforms for the forward).  The analytic choice
+// minimises it; the autotuner may override it for the view count it tuned.
+int best_chunk(const spect_plan_s* p, int nv, double c0) {
+  double best = 1e300;
+  int bc = p->ny;
+  for (int cy = 1; cy <= p->ny; ++cy) {
+    const int nc = cdiv(p->ny, cy);
+    if (nc > p->nchunk_max) continue;
+    const double waves = std::ceil((double)nv * nc / p->conv_grid);
+    const double cost = waves * (cy + c0);
+    if (cost < best - 1e-9) {
+      best = cost;
+      bc = cy;
+    }
+  }
+  return bc;
+}
+
+void chunking(const spect_plan_s* p, int nv, bool adj, int* chunkY, int* nchunks) {
+  int cy = 0;
+  if (p->tuned_nv == nv) cy = adj ? p->tune_adj_cy : p->tune_fwd_cy;
+  if (cy <= 0) cy = best_chunk(p, std::max(nv, 1), adj ? 0.25 : 1.0);
   *chunkY = cy;
   *nchunks = cdiv(p->ny, cy);
 }
@@ -378,16 +456,22 @@ Conv2Args conv_args(const spect_plan_s* p) {
   a.gacc = p->d_gacc;
   a.tw = p->d_tw;
   a.bsmem = p->conv_bsmem;
+  // :two with the cache: the attenuation is applied inside the convolution kernels
+  a.att = p->d_att;
+  a.att_mul = (p->d_att && p->interp == SPECT_INTERP_TWO) ? 1 : 0;
+  a.err = p->d_err;
   return a;
 }
 
-cudaError_t conv_launch(const spect_plan_s* p, int kind, int grid, cudaStream_t st, const Conv2Args& a) {
+cudaError_t conv_launch(const spect_plan_s* p, int kind, int grid, cudaStream_t st, const Conv2Args& a,
+                        size_t smem = 0) {
+  if (!smem) smem = p->conv_smem;
   switch (p->RX) {
-    case 1: return conv2_launch_rx1(kind, p->RZ, grid, p->conv_smem, st, a);
-    case 2: return conv2_launch_rx2(kind, p->RZ, grid, p->conv_smem, st, a);
-    case 4: return conv2_launch_rx4(kind, p->RZ, grid, p->conv_smem, st, a);
-    case 8: return conv2_launch_rx8(kind, p->RZ, grid, p->conv_smem, st, a);
-    case 16: return conv2_launch_rx16(kind, p->RZ, grid, p->conv_smem, st, a);
+    case 1: return conv2_launch_rx1(kind, p->RZ, grid, smem, st, a);
+    case 2: return conv2_launch_rx2(kind, p->RZ, grid, smem, st, a);
+    case 4: return conv2_launch_rx4(kind, p->RZ, grid, smem, st, a);
+    case 8: return conv2_launch_rx8(kind, p->RZ, grid, smem, st, a);
+    case 16: return conv2_launch_rx16(kind, p->RZ, grid, smem, st, a);
   }
   return cudaErrorInvalidValue;
 }
@@ -403,6 +487,7 @@ int forward_scratch(spect_plan_s* p, float* views, const float* image, const int
     // rotation + attenuation -> P
     int vpb = p->rotf_vpb;
     int nsplit = std::max(1, std::min(cdiv(2 * p->sm_count, g.nz), cdiv(nv, vpb)));
+    if (p->tuned_nv == nv && p->tune_rotf_nsplit > 0) nsplit = std::min(p->tune_rotf_nsplit, cdiv(nv, vpb));
     dim3 grid(g.nz, nsplit);
     const int thr = g.nx * vpb;
     const float* att = p->d_att;
@@ -429,7 +514,7 @@ int forward_scratch(spect_plan_s* p, float* views, const float* image, const int
     // FFT convolution + depth sum -> part
     Conv2Args a = conv_args(p);
     int cy, nc;
-    chunking(p, nv, &cy, &nc);
+    chunking(p, nv, false, &cy, &nc);
     a.P = Pbuf;
     a.vidx = vi;
     a.nv = nv;
@@ -437,7 +522,8 @@ int forward_scratch(spect_plan_s* p, float* views, const float* image, const int
     a.nchunks = nc;
     a.part = partbuf;
     int gridc = std::min(p->conv_grid, nv * nc);
-    LAUNCH(p, K_CONV_FWD, st, "k_conv_fwd", conv_launch(p, 0, gridc, st, a));
+    LAUNCH(p, K_CONV_FWD, st, "k_conv_fwd",
+           conv_launch(p, p->conv_stage ? 3 : 0, gridc, st, a, p->conv_stage ? p->conv_smem_fwd : p->conv_smem));
     // chunk sum (+ EM ratio) -> views
     size_t n = (size_t)nv * p->nxz;
     int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16);
@@ -472,12 +558,13 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     a.vidx = vi;
     LAUNCH(p, K_VSPEC, st, "k_vspec", conv_launch(p, 2, std::min(p->conv_grid, nv), st, a));
     int cy, nc;
-    chunking(p, nv, &cy, &nc);
+    chunking(p, nv, true, &cy, &nc);
     a.Vs = p->d_Vs;
     a.T = p->d_P;
     a.chunkY = cy;
     a.nchunks = nc;
-    LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj", conv_launch(p, 1, std::min(p->conv_grid, nv * nc), st, a));
+    LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj",
+           conv_launch(p, p->adj_stage ? 4 : 1, std::min(p->conv_grid, nv * nc), st, a, p->conv_smem_adj));
     dim3 grid(g.nz, nsplit);
     const size_t rsm = p->rota_smem_ok ? p->rota_smem : 0;
     if (p->interp == SPECT_INTERP_ONE) {
@@ -490,12 +577,18 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
                  p->r1, p->d_R1, p->d_r1view, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->r1a_smem_ok, p->d_gscr_r1));
     } else
     LAUNCH(p, K_ROT_ADJ, st, "k_rot_adj",
-           if (p->d_att) k_rot_adj<true><<<grid, kRotAdjThreads, rsm, st>>>(
+           if (p->adj_stage == 2) k_rot_adj_band<<<dim3(g.nz, nsplit, p->rot_nband), kRotAdjThreads,
+                                                   p->rota_smem_stage, st>>>(
+               g, p->d_P, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rot_nband, p->d_err);
+           else if (p->adj_stage == 1) k_rot_adj<true, true><<<grid, kRotAdjThreads, p->rota_smem_stage, st>>>(
+               g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, 1, p->d_gscr_adj,
+               p->d_err);
+           else if (p->d_att) k_rot_adj<true, false><<<grid, kRotAdjThreads, rsm, st>>>(
                g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
-               p->d_gscr_adj);
-           else k_rot_adj<false><<<grid, kRotAdjThreads, rsm, st>>>(
+               p->d_gscr_adj, p->d_err);
+           else k_rot_adj<false, false><<<grid, kRotAdjThreads, rsm, st>>>(
                g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
-               p->d_gscr_adj));
+               p->d_gscr_adj, p->d_err));
   }
   int rb = (int)std::min<size_t>((p->N + 255) / 256, (size_t)p->sm_count * 16);
   LAUNCH(p, K_REDUCE_IMAGE, st, "k_reduce_image",
@@ -638,6 +731,124 @@ int static_scratch_address(void** out) {
   return SPECT_OK;
 }
 
+// ------------------------------------------------------------------------
+// Autotuner: times candidate launch shapes of the forward and adjoint
+// projector for nv views on the plan's own buffers and keeps the fastest;
+// results are cached per plan shape for the process.
+struct TuneResult {
+  int fwd_cy, adj_cy, rotf_nsplit, nsplit_adj;
+  double fwd_ms, adj_ms;
+};
+std::mutex g_tune_mu;
+std::vector<std::pair<std::string, TuneResult>> g_tune_cache;
+
+std::string tune_key(const spect_plan_s* p, int nv) {
+  return std::to_string(p->nx) + "x" + std::to_string(p->nz) + "/" + std::to_string(p->px) + "x" +
+         std::to_string(p->pz) + "/v" + std::to_string(p->nview) + "/n" + std::to_string(nv) + "/i" +
+         std::to_string(p->interp) + "/a" + std::to_string(p->d_att ? 1 : 0) + "/d" + std::to_string(p->device);
+}
+
+int time_pass(spect_plan_s* p, bool adj, int nv, int reps, double* ms) {
+  cudaStream_t st = p->home;
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  double best = 1e300;
+  int rc = SPECT_OK;
+  for (int r = 0; r <= reps && rc == SPECT_OK; ++r) {  // r = 0: warm-up
+    cudaEventRecord(a, st);
+    rc = adj ? backward(p, p->d_io_img, p->d_io_views, p->d_all, nv, st, 0, nullptr)
+             : forward(p, p->d_io_views, p->d_io_img, p->d_all, nv, st, nullptr, nullptr);
+    cudaEventRecord(b, st);
+    if (cudaEventSynchronize(b) != cudaSuccess) rc = fail(SPECT_ERR_CUDA, "autotune timing");
+    float t = 0;
+    cudaEventElapsedTime(&t, a, b);
+    if (r > 0) best = std::min(best, (double)t);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = best;
+  return rc;
+}
+
+int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
+  const std::string key = tune_key(p, nv);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (auto& kv : g_tune_cache)
+      if (kv.first == key) {
+        p->tuned_nv = nv;
+        p->tune_fwd_cy = kv.second.fwd_cy;
+        p->tune_adj_cy = kv.second.adj_cy;
+        p->tune_rotf_nsplit = kv.second.rotf_nsplit;
+        p->nsplit_adj = kv.second.nsplit_adj;
+        *fwd_ms = kv.second.fwd_ms;
+        *adj_ms = kv.second.adj_ms;
+        return SPECT_OK;
+      }
+  }
+  STATUS_TRY(ensure_io(p));
+  {
+    std::vector<float> h(std::max(p->N, (size_t)nv * p->nxz), 1.0f);
+    STATUS_TRY(upload(p, p->d_io_img, h.data(), sizeof(float) * p->N));
+    STATUS_TRY(upload(p, p->d_io_views, h.data(), sizeof(float) * (size_t)nv * p->nxz));
+  }
+  const bool prof = p->prof.on;
+  p->prof.on = false;
+  p->tuned_nv = nv;
+  // candidate depth tiles: the analytic optimum for a few overhead weights
+  std::vector<int> cys;
+  for (double c0 : {0.0, 0.25, 0.5, 1.0, 2.0, 4.0}) {
+    int c = best_chunk(p, nv, c0);
+    if (std::find(cys.begin(), cys.end(), c) == cys.end()) cys.push_back(c);
+  }
+  // forward: depth tile x rotation split
+  std::vector<int> rsplits = {0};
+  for (int f : {1, 2, 4, 8})
+    if (f * p->g.nz <= 8 * p->sm_count) rsplits.push_back(f);
+  double bf = 1e300;
+  int bcy = cys[0], brs = 0, rc = SPECT_OK;
+  for (int cy : cys)
+    for (int rs : rsplits) {
+      p->tune_fwd_cy = cy;
+      p->tune_rotf_nsplit = rs;
+      double t;
+      if ((rc = time_pass(p, false, nv, 2, &t)) != SPECT_OK) break;
+      if (t < bf) {
+        bf = t;
+        bcy = cy;
+        brs = rs;
+      }
+    }
+  p->tune_fwd_cy = bcy;
+  p->tune_rotf_nsplit = brs;
+  // adjoint: depth tile x view split of the rotation adjoint
+  double ba = 1e300;
+  int bacy = cys[0], bns = p->nsplit_adj;
+  for (int cy : cys)
+    for (int ns : {1, 2, 4, 8, 16}) {
+      if (rc != SPECT_OK || ns > p->nsplit_adj_max) break;
+      p->tune_adj_cy = cy;
+      p->nsplit_adj = ns;
+      double t;
+      if ((rc = time_pass(p, true, nv, 2, &t)) != SPECT_OK) break;
+      if (t < ba) {
+        ba = t;
+        bacy = cy;
+        bns = ns;
+      }
+    }
+  p->tune_adj_cy = bacy;
+  p->nsplit_adj = bns;
+  p->prof.on = prof;
+  if (rc != SPECT_OK) return rc;
+  *fwd_ms = bf;
+  *adj_ms = ba;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache.push_back({key, TuneResult{bcy, bacy, brs, bns, bf, ba}});
+  return SPECT_OK;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------------
@@ -737,7 +948,43 @@ struct PlanOpts {
   bool async_alloc = false;
   int gmax_cap = 0;     // > 0: at most this many views per group (scratch bound)
   int atten_cache = -1; // -1 auto, 0 off (:two only), 1 on
+  // compact PSFs: psfs holds nset distinct [ny][pz][px] stacks and
+  // view_set[v] names the stack of view v (already checked for symmetry)
+  const int* view_set = nullptr;
+  int nset = 0;
 };
+
+// distinct PSF stacks of nview views (stack = ny*pp floats each): view_set[v]
+// is the index into uniq (the first view of each distinct stack)
+void psf_sets(const float* psfs, int nview, size_t stack, std::vector<int>& view_set, std::vector<int>& uniq) {
+  view_set.assign(nview, 0);
+  uniq.clear();
+  for (int v = 0; v < nview; ++v) {
+    int found = -1;
+    for (size_t u = 0; u < uniq.size(); ++u)
+      if (std::memcmp(psfs + (size_t)uniq[u] * stack, psfs + (size_t)v * stack, sizeof(float) * stack) == 0) {
+        found = (int)u;
+        break;
+      }
+    if (found < 0) {
+      found = (int)uniq.size();
+      uniq.push_back(v);
+    }
+    view_set[v] = found;
+  }
+}
+
+// every px x pz plane of the given stacks point-symmetric (src/spectplan.jl:84-88)
+bool psf_symmetric(const float* psfs, const std::vector<int>& stacks, size_t ny, size_t pp) {
+  for (int u : stacks)
+    for (size_t y = 0; y < ny; ++y) {
+      const float* k = psfs + ((size_t)u * ny + y) * pp;
+      for (size_t i = 0; i < pp / 2; ++i)
+        if (!(k[i] == k[pp - 1 - i])) return false;
+      if (!(k[pp / 2] == k[pp / 2])) return false;  // a NaN centre is not symmetric
+    }
+  return true;
+}
 
 int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview, const float* mumap,
                      const float* psfs, float dy, const float* viewangle, int interpmeth, int mode, int nthread,
@@ -751,10 +998,15 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
   if ((nx % 2) || (ny % 2)) return fail(SPECT_ERR_NX_ODD, "nx odd");
   if (!(px % 2) || !(pz % 2)) return fail(SPECT_ERR_PSF_NOT_ODD, "non-odd size psfs");
   const size_t pp = (size_t)px * pz;
-  for (size_t pl = 0; pl < (size_t)ny * nview; ++pl) {
-    const float* k = psfs + pl * pp;
-    for (size_t i = 0; i < pp; ++i)
-      if (!(k[i] == k[pp - 1 - i])) return fail(SPECT_ERR_PSF_ASYM, "asym. psf");
+  // distinct PSF stacks first: identical stacks are symmetric together
+  const size_t stack = (size_t)ny * pp;
+  std::vector<int> view_set, uniq;
+  if (opts.view_set) {
+    view_set.assign(opts.view_set, opts.view_set + nview);
+    for (int u = 0; u < opts.nset; ++u) uniq.push_back(u);  // stack u of the compact array
+  } else {
+    psf_sets(psfs, nview, stack, view_set, uniq);
+    if (!psf_symmetric(psfs, uniq, ny, pp)) return fail(SPECT_ERR_PSF_ASYM, "asym. psf");
   }
   if (interpmeth != SPECT_INTERP_ONE && interpmeth != SPECT_INTERP_TWO)
     return fail(SPECT_ERR_INTERP, "bad interpmeth");
@@ -830,23 +1082,7 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     bool ident = std::fmod((double)p->angles[v], kTwoPi) == 0.0;
     rot[v] = make_float4((float)std::cos(phi), (float)std::sin(phi), ident ? 1.f : 0.f, p->angles[v]);
   }
-  // distinct PSF stacks
-  const size_t stack = (size_t)ny * pp;
-  std::vector<int> uniq;
-  p->view_set.resize(nview);
-  for (int v = 0; v < nview; ++v) {
-    int found = -1;
-    for (size_t u = 0; u < uniq.size(); ++u)
-      if (std::memcmp(psfs + (size_t)uniq[u] * stack, psfs + (size_t)v * stack, sizeof(float) * stack) == 0) {
-        found = (int)u;
-        break;
-      }
-    if (found < 0) {
-      found = (int)uniq.size();
-      uniq.push_back(v);
-    }
-    p->view_set[v] = found;
-  }
+  p->view_set = view_set;
   p->nset = (int)uniq.size();
 
   // group size: rotated-plane scratch bounded by ~1 GiB
@@ -856,12 +1092,15 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
 
   if ((st = dalloc(p, &p->d_mumap, p->N)) || (st = dalloc(p, &p->d_rot, nview)) ||
       (st = dalloc(p, &p->d_viewset, nview)) || (st = dalloc(p, &p->d_tw, SPECT_TW_N)) ||
-      (st = dalloc(p, &p->d_all, nview)) || (st = dalloc(p, &p->d_idx, nview)) ||
+      (st = dalloc(p, &p->d_all, nview)) || (st = dalloc(p, &p->d_idx, nview)) || (st = dalloc(p, &p->d_err, 1)) ||
+      (st = (cudaMemsetAsync(p->d_err, 0, sizeof(int), p->home) == cudaSuccess) ? SPECT_OK
+                                                                                 : fail(SPECT_ERR_CUDA, "memset")) ||
       (st = dalloc(p, &p->d_H, (size_t)p->nset * ny * (p->cg.Q + 1) * Npx)) ||
       (st = dalloc(p, &p->d_P, (size_t)p->gmax * p->N)) ||
-      (st = dalloc(p, &p->d_part, (size_t)p->gmax * p->nchunk_max * p->nxz)) ||
+      (st = ((p->nchunk_max = ((size_t)p->gmax * 32 * p->nxz * 4 <= ((size_t)256 << 20)) ? 32 : 16),
+             dalloc(p, &p->d_part, (size_t)p->gmax * p->nchunk_max * p->nxz))) ||
       (st = dalloc(p, &p->d_Vs, (size_t)p->gmax * p->cg.Q * Npx)) ||
-      (st = dalloc(p, &p->d_imgpart, (size_t)p->nsplit_adj * p->N)))
+      (st = dalloc(p, &p->d_imgpart, (size_t)p->nsplit_adj_max * p->N)))
     return bail(st);
 
   std::vector<float2> tw(SPECT_TW_N);
@@ -897,7 +1136,7 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     p->r1_grid_y = std::max(1, cdiv(4 * p->sm_count, nz));
     size_t gs = 0;
     if (!p->r1f_smem_ok) gs = std::max(gs, (size_t)nz * p->r1_grid_y * (p->r1f_smem / sizeof(float)));
-    if (!p->r1a_smem_ok) gs = std::max(gs, (size_t)nz * p->nsplit_adj * (p->r1a_smem / sizeof(float)));
+    if (!p->r1a_smem_ok) gs = std::max(gs, (size_t)nz * p->nsplit_adj_max * (p->r1a_smem / sizeof(float)));
     if (gs && (st = dalloc(p, &p->d_gscr_r1, gs))) return bail(st);
     if ((st = dalloc(p, &p->d_R1, (size_t)p->gmax * p->N)) || (st = dalloc(p, &p->d_r1view, nview)))
       return bail(st);
@@ -1086,6 +1325,19 @@ int spect_project_static_scratch(spect_plan_t p, float* views, const float* imag
   return rc;
 }
 
+// end of a host-synchronous call: wait for the stream, then report a kernel
+// whose bounded wait on a bulk copy gave up (the flag is cleared)
+int host_done(spect_plan_s* p, cudaStream_t st) {
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) {
+    CUDA_TRY(cudaMemset(p->d_err, 0, sizeof(int)));
+    return fail(SPECT_ERR_TIMEOUT, "a bulk copy into shared memory did not complete");
+  }
+  return SPECT_OK;
+}
+
 int spect_project_host(spect_plan_t p, float* views, const float* image, const int32_t* index, int nindex) {
   if (!p || !views || !image) return fail(SPECT_ERR_ARG, "null pointer argument");
   std::lock_guard<std::mutex> lk(p->mu);
@@ -1096,8 +1348,7 @@ int spect_project_host(spect_plan_t p, float* views, const float* image, const i
   CUDA_TRY(cudaMemcpyAsync(p->d_io_img, image, sizeof(float) * p->N, cudaMemcpyHostToDevice, st));
   STATUS_TRY(forward(p, p->d_io_views, p->d_io_img, vi, nindex, st, nullptr, nullptr));
   CUDA_TRY(cudaMemcpyAsync(views, p->d_io_views, sizeof(float) * nindex * p->nxz, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  return SPECT_OK;
+  return host_done(p, st);
 }
 
 int spect_backproject(spect_plan_t p, float* image, const float* views, const int32_t* index, int nindex,
@@ -1120,8 +1371,7 @@ int spect_backproject_host(spect_plan_t p, float* image, const float* views, con
   CUDA_TRY(cudaMemcpyAsync(p->d_io_views, views, sizeof(float) * nindex * p->nxz, cudaMemcpyHostToDevice, st));
   STATUS_TRY(backward(p, p->d_io_img, p->d_io_views, vi, nindex, st, 0, nullptr));
   CUDA_TRY(cudaMemcpyAsync(image, p->d_io_img, sizeof(float) * p->N, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  return SPECT_OK;
+  return host_done(p, st);
 }
 
 int spect_osem(spect_plan_t p, float* out, const float* x0, const float* ynoisy, const float* background, int nblocks,
@@ -1153,8 +1403,7 @@ int spect_osem_host(spect_plan_t p, float* out, const float* x0, const float* yn
   CUDA_TRY(cudaMemcpyAsync(db, background, sizeof(float) * V, cudaMemcpyHostToDevice, st));
   STATUS_TRY(run_osem(p, dx, dx, dy, db, nblocks, niter, st));
   CUDA_TRY(cudaMemcpyAsync(out, dx, sizeof(float) * p->N, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  return SPECT_OK;
+  return host_done(p, st);
 }
 
 int spect_mlem_host(spect_plan_t p, float* out, const float* x0, const float* ynoisy, const float* background,
@@ -1208,6 +1457,9 @@ int spect_batch_create(spect_batch_t* out, int njobs, const spect_plan_t* plans,
   for (int j = 0; j < njobs; ++j) {
     std::lock_guard<std::mutex> lk(b->plans[j]->mu);
     int st = prepare_osem(b->plans[j], nblocks[j], niter[j]);
+    double f, a;
+    if (st == SPECT_OK && (b->plans[j]->nview % nblocks[j]) == 0)
+      st = autotune(b->plans[j], b->plans[j]->nview / nblocks[j], &f, &a);
     if (st != SPECT_OK) return bail(st);
   }
   if (cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1265,6 +1517,18 @@ int spect_batch_destroy(spect_batch_t b) {
   if (b->root) cudaStreamDestroy(b->root);
   if (b->fork) cudaEventDestroy(b->fork);
   delete b;
+  return SPECT_OK;
+}
+
+int spect_plan_autotune(spect_plan_t p, int nindex, double ms[2]) {
+  if (!p || nindex < 1 || nindex > p->nview) return fail(SPECT_ERR_ARG, "bad spect_plan_autotune arguments");
+  std::lock_guard<std::mutex> lk(p->mu);
+  double f = 0, a = 0;
+  STATUS_TRY(autotune(p, nindex, &f, &a));
+  if (ms) {
+    ms[0] = f;
+    ms[1] = a;
+  }
   return SPECT_OK;
 }
 
@@ -1343,7 +1607,8 @@ struct ServerJob {
   long long ticket = 0;
   int nx = 0, nz = 0, px = 0, pz = 0, nview = 0, interp = 2, nblocks = 1, niter = 1;
   float dy = 1.f;
-  std::vector<float> mumap, psfs, y, bg, x0, result;
+  std::vector<float> mumap, psfs, y, bg, x0, result;  // psfs: the distinct stacks only
+  std::vector<int> view_set;                          // view -> stack of psfs
   int state = 0;  // 0 pending, 1 active, 2 done, 3 failed
   int status = SPECT_OK;
   std::string err;
@@ -1370,10 +1635,15 @@ size_t est_job_bytes(const ServerJob& j, bool att) {
   // per-CTA global slabs of large planes (B, spectra accumulators)
   if ((size_t)j.nx * (Q + 1) * 8 + 8192 > 227 * 1024) b += (size_t)148 * j.nx * (Q + 1) * 8;
   if ((Npx / std::min(32, Npx)) * (Npz / std::min(32, Npz)) > 32) b += (size_t)148 * Q * Npx * 8;
+  const size_t slice = (size_t)j.nx * j.nx;
+  if ((2 * slice + 4 * (size_t)j.nx) * 4 > 227 * 1024) b += (size_t)j.nz * 8 * (2 * slice + 512) * 4;
+  if (j.nx * 32 * nxz * 4 > ((size_t)256 << 20)) b += 0;  // part stays at 16 chunks
   return b + b / 10 + ((size_t)16 << 20);
 }
 
 }  // namespace
+
+constexpr int kServerThreads = 4;
 
 struct spect_server_s {
   size_t budget = 0;
@@ -1388,9 +1658,10 @@ struct spect_server_s {
   size_t used = 0;
   bool stop = false;
   long long n_submitted = 0, n_done = 0, n_failed = 0, max_active_seen = 0;
-  float* staging = nullptr;  // pinned result staging
-  size_t staging_n = 0;
-  std::thread worker;
+  // scheduler threads: each admits and retires jobs; while one prepares a
+  // job's plan on the host (validation, uploads, PSF spectra) the others
+  // keep admitting and retiring
+  std::vector<std::thread> workers;
 };
 
 namespace {
@@ -1422,6 +1693,8 @@ int job_admit(ServerJob* j, size_t budget) {
   o.gmax_cap = j->nview / j->nblocks;
   const size_t att = sizeof(float) * (size_t)j->nx * j->nx * j->nz * j->nview;
   o.atten_cache = (j->interp == SPECT_INTERP_ONE || att <= budget / 8) ? 1 : 0;
+  o.view_set = j->view_set.data();
+  o.nset = (int)(j->psfs.size() / ((size_t)j->nx * j->px * j->pz));
   spect_plan_t plan = nullptr;
   STATUS_TRY(plan_create_impl(&plan, j->nx, j->nx, j->nz, j->px, j->pz, j->nview, j->mumap.data(), j->psfs.data(),
                               j->dy, nullptr, j->interp, SPECT_MODE_FAST, 1, 1, o));
@@ -1444,6 +1717,8 @@ int job_admit(ServerJob* j, size_t budget) {
 
 void server_loop(spect_server_s* S) {
   cudaSetDevice(S->device);
+  float* staging = nullptr;  // this thread's pinned result staging
+  size_t staging_n = 0;
   std::unique_lock<std::mutex> lk(S->mu);
   for (;;) {
     // completions
@@ -1456,18 +1731,17 @@ void server_loop(spect_server_s* S) {
       }
       const size_t N = j->plan ? j->plan->N : 0;
       if (q == cudaSuccess) {
-        if (S->staging_n < N) {
-          if (S->staging) cudaFreeHost(S->staging);
-          S->staging = nullptr;
-          S->staging_n = 0;
-          if (cudaMallocHost((void**)&S->staging, sizeof(float) * N) == cudaSuccess) S->staging_n = N;
+        if (staging_n < N) {
+          if (staging) cudaFreeHost(staging);
+          staging = nullptr;
+          staging_n = 0;
+          if (cudaMallocHost((void**)&staging, sizeof(float) * N) == cudaSuccess) staging_n = N;
         }
-        cudaError_t e = S->staging ? cudaMemcpyAsync(S->staging, j->d_x, sizeof(float) * N, cudaMemcpyDeviceToHost,
-                                                     j->st)
-                                   : cudaErrorMemoryAllocation;
+        cudaError_t e = staging ? cudaMemcpyAsync(staging, j->d_x, sizeof(float) * N, cudaMemcpyDeviceToHost, j->st)
+                                : cudaErrorMemoryAllocation;
         if (e == cudaSuccess) e = cudaStreamSynchronize(j->st);
         if (e == cudaSuccess) {
-          j->result.assign(S->staging, S->staging + N);
+          j->result.assign(staging, staging + N);
           j->state = 2;
           S->n_done++;
         } else {
@@ -1526,7 +1800,7 @@ void server_loop(spect_server_s* S) {
       S->max_active_seen = std::max<long long>(S->max_active_seen, (long long)S->active.size());
     }
     if (S->stop && S->active.empty()) break;
-    if (S->active.empty()) {
+    if (S->active.empty() && S->pending.empty()) {
       S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
     } else {
       lk.unlock();
@@ -1534,6 +1808,8 @@ void server_loop(spect_server_s* S) {
       lk.lock();
     }
   }
+  lk.unlock();
+  if (staging) cudaFreeHost(staging);
 }
 
 }  // namespace
@@ -1552,7 +1828,7 @@ int spect_server_create(spect_server_t* out, size_t device_budget, int max_activ
   if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) fr = 0;
   S->budget = device_budget ? device_budget : fr / 2;
   S->max_active = max_active;
-  S->worker = std::thread(server_loop, S);
+  for (int t = 0; t < kServerThreads; ++t) S->workers.emplace_back(server_loop, S);
   *out = S;
   return SPECT_OK;
 }
@@ -1569,13 +1845,12 @@ int spect_server_submit(spect_server_t S, const spect_job_desc* d, long long* ti
   if (d->nblocks < 1 || d->nview % d->nblocks != 0) return fail(SPECT_ERR_NBLOCKS, "nview must be divisible by nblocks!");
   if (d->niter < 0) return fail(SPECT_ERR_ARG, "niter must be >= 0");
   const size_t N = (size_t)d->nx * d->nx * d->nz, V = (size_t)d->nx * d->nz * d->nview;
-  const size_t P = (size_t)d->px * d->pz * d->nx * d->nview;
   for (size_t k = 0; k < V; ++k)
     if (!(d->background[k] > 0.f)) return fail(SPECT_ERR_BACKGROUND, "need background > 0");
-  const size_t pp = (size_t)d->px * d->pz;
-  for (size_t pl = 0; pl < P / pp; ++pl)
-    for (size_t i = 0; i < pp; ++i)
-      if (!(d->psfs[pl * pp + i] == d->psfs[pl * pp + pp - 1 - i])) return fail(SPECT_ERR_PSF_ASYM, "asym. psf");
+  const size_t pp = (size_t)d->px * d->pz, stack = (size_t)d->nx * pp;
+  std::vector<int> view_set, uniq;
+  psf_sets(d->psfs, d->nview, stack, view_set, uniq);
+  if (!psf_symmetric(d->psfs, uniq, d->nx, pp)) return fail(SPECT_ERR_PSF_ASYM, "asym. psf");
   if (power2(d->nx + d->px - 1) > SPECT_TW_N || power2(d->nz + d->pz - 1) > SPECT_TW_N)
     return fail(SPECT_ERR_UNSUPPORTED, "padded plane exceeds this build's FFT limit");
   ServerJob* j = new ServerJob;
@@ -1589,7 +1864,10 @@ int spect_server_submit(spect_server_t S, const spect_job_desc* d, long long* ti
   j->niter = d->niter;
   j->dy = d->dy;
   j->mumap.assign(d->mumap, d->mumap + N);
-  j->psfs.assign(d->psfs, d->psfs + P);
+  j->psfs.resize(uniq.size() * stack);
+  for (size_t u = 0; u < uniq.size(); ++u)
+    std::memcpy(j->psfs.data() + u * stack, d->psfs + (size_t)uniq[u] * stack, sizeof(float) * stack);
+  j->view_set = std::move(view_set);
   j->y.assign(d->ynoisy, d->ynoisy + V);
   j->bg.assign(d->background, d->background + V);
   if (d->x0) j->x0.assign(d->x0, d->x0 + N);
@@ -1655,9 +1933,9 @@ int spect_server_destroy(spect_server_t S) {
     S->pending.clear();
   }
   S->cv_work.notify_all();
-  if (S->worker.joinable()) S->worker.join();  // running jobs finish first
+  for (auto& w : S->workers)
+    if (w.joinable()) w.join();  // running jobs finish first
   for (auto& kv : S->jobs) delete kv.second;
-  if (S->staging) cudaFreeHost(S->staging);
   delete S;
   return SPECT_OK;
 }

@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "bulk_copy.cuh"
+
 
 namespace spect {
 
@@ -144,13 +146,14 @@ __global__ void __launch_bounds__(1024) k_rot_fwd(Geom g, const float* __restric
     const bool ident = r.z != 0.f;
     float prefix = 0.f;
     float* out = P + ((size_t)s * ny * nz + z) * nx + x;
-    const float* av = att + ((size_t)v * ny * nz + z) * nx + x;
 #pragma unroll 8
     for (int y = 0; y < ny; ++y) {
       const float f = ident ? img[x + y * nx] : bilinear(img, nx, R, x, y);
       float a;
       if (CACHED) {
-        a = __ldg(av + (size_t)y * nz * nx);
+        // the convolution kernel applies the cached attenuation on load
+        out[(size_t)y * nz * nx] = f;
+        continue;
       } else {
         const float m = ident ? mu[x + y * nx] : bilinear(mu, nx, R, x, y);
         // exp(-dy * (sum_{j<y} mu_j + mu_y/2))  (src/project.jl:103-113)
@@ -189,16 +192,20 @@ __global__ void k_reduce_views(const float* __restrict__ part, int nv, int nchun
 // CACHED: a_s from the attenuation cache; otherwise rotated mu-map + depth
 // scan per view (imrotate! of the mu-map and the attenuation of
 // src/backproject.jl:285-317).
+// STAGE (with CACHED): T already carries a_s (the adjoint convolution
+// multiplied it in); each slot's slice rows are bulk-copied into one of two
+// shared buffers while the previous slot is scattered.  Shared memory:
+// acc, two slices, two mbarriers.
 constexpr int kRotAdjThreads = 512;
 
-template <bool CACHED>
+template <bool CACHED, bool STAGE>
 __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const float* __restrict__ T,
                                                                 const float* __restrict__ mumap,
                                                                 const float* __restrict__ att,
                                                                 const float4* __restrict__ rot,
                                                                 const int* __restrict__ vidx, int nv,
                                                                 float* __restrict__ imgpart, int accumulate,
-                                                                int use_smem, float* __restrict__ gscr) {
+                                                                int use_smem, float* __restrict__ gscr, int* err) {
   extern __shared__ float4 smem4[];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int z = blockIdx.x, split = blockIdx.y;
@@ -226,13 +233,53 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
   const float mdy = -g.dy;
   const int seglen = (ny + nseg - 1) / nseg;
   const int myseg = threadIdx.x / nx, o1s = threadIdx.x - myseg * nx;
+  float* Sb[2] = {S, S + slice};
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(S + 2 * slice);
+  unsigned phase[2] = {0u, 0u};
+  // warp 0: rows y of slot sl's slice z into buffer b
+  auto issue = [&](int sl, int b) {
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect(&bar[b], (unsigned)(slice * sizeof(float)));
+    }
+    __syncwarp();
+    fence_proxy_async();
+    for (int y = lane; y < ny; y += 32)
+      bulk_copy(&bar[b], Sb[b] + (size_t)y * nx, T + (((size_t)sl * ny + y) * nz + z) * nx,
+                (unsigned)(nx * sizeof(float)));
+  };
+  if (STAGE) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar[0]);
+      mbar_init(&bar[1]);
+    }
+    __syncthreads();
+    if (warp == 0 && s0 < s1) issue(s0, 0);
+  }
   for (int s = s0; s < s1; ++s) {
     const int v = vidx[s];
     const float4 r = rot[v];
     RotPos R{r.x, r.y, g.c0};
     const bool ident = r.z != 0.f;
-    __syncthreads();
-    if (CACHED) {
+    const int b = (s - s0) & 1;
+    if (STAGE) {
+      // this slot's rows have landed; the block barrier also ends the
+      // previous slot's scatter, so the other buffer is free
+      if (__syncthreads_or(!mbar_wait(&bar[b], phase[b]))) {
+        if (threadIdx.x == 0) {
+          atomicExch(err, 1);
+          mbar_wait(&bar[b], phase[b]);
+        }
+        return;
+      }
+      phase[b] ^= 1u;
+      S = Sb[b];
+      if (warp == 0 && s + 1 < s1) issue(s + 1, b ^ 1);
+    } else {
+      __syncthreads();
+    }
+    if (STAGE) {
+    } else if (CACHED) {
       // S = a .* T on the rotated grid (coalesced rows of x)
       const float* av = att + ((size_t)v * ny * nz + z) * nx;
       const float* tv = T + ((size_t)s * ny * nz + z) * nx;
@@ -297,6 +344,136 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
   }
   __syncthreads();
   for (int k = threadIdx.x; k < slice; k += blockDim.x) outp[k] = acc[k];
+}
+
+// k_rot_adj_band: the adjoint rotation for slices too large for shared
+// memory.  grid (nz, nsplit, nband): each block owns a band of output rows of
+// slice z (its accumulator stays in shared memory) and streams the
+// premultiplied slices T of its slots through two shared buffers of
+// kRotBandRows rows (bulk copies).  Chunks of rows whose rotated positions
+// cannot reach the band are skipped.  The 9-class scatter is that of
+// k_rot_adj, restricted to taps inside the band.
+constexpr int kRotBandRows = 32;
+
+__global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, const float* __restrict__ T,
+                                                                     const float4* __restrict__ rot,
+                                                                     const int* __restrict__ vidx, int nv,
+                                                                     float* __restrict__ imgpart, int accumulate,
+                                                                     int nband, int* err) {
+  extern __shared__ float4 smem4[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int z = blockIdx.x, split = blockIdx.y;
+  const int rows = (ny + nband - 1) / nband;
+  const int ya = blockIdx.z * rows, yb = min(ny, ya + rows);
+  if (ya >= yb) return;  // uniform over the block
+  constexpr int CH = kRotBandRows;
+  const int nch = (ny + CH - 1) / CH;
+  float* acc = reinterpret_cast<float*>(smem4);
+  float* Sb[2] = {acc + (size_t)rows * nx, acc + (size_t)rows * nx + (size_t)CH * nx};
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(Sb[1] + (size_t)CH * nx);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* outp = imgpart + (((size_t)split * nz + z) * ny + ya) * nx;
+  const int nel = (yb - ya) * nx;
+  for (int k = threadIdx.x; k < nel; k += blockDim.x) acc[k] = accumulate ? outp[k] : 0.f;
+  const int per = (nv + gridDim.y - 1) / gridDim.y;
+  const int s0 = split * per, s1 = min(nv, s0 + per);
+  const float c0 = g.c0;
+  // can rows [c*CH, c*CH + CH) of slot s reach rows [ya, yb)?  s2 is affine
+  // in (o1, o2): bound it by the corners, with a one-pixel margin
+  auto reach = [&](int s, int c) -> bool {
+    const float4 r = rot[vidx[s]];
+    const float r0 = (float)(c * CH), r1 = (float)(min(ny, c * CH + CH) - 1);
+    const float a0 = r.y * (0.f - c0), a1 = r.y * ((float)(nx - 1) - c0);
+    const float b0 = r.x * (r0 - c0), b1 = r.x * (r1 - c0);
+    const float lo = c0 + fminf(a0, a1) + fminf(b0, b1), hi = c0 + fmaxf(a0, a1) + fmaxf(b0, b1);
+    return hi > (float)ya - 2.f && lo < (float)yb + 1.f;
+  };
+  auto next = [&](int& s, int& c) {
+    for (;;) {
+      if (++c >= nch) {
+        c = 0;
+        ++s;
+      }
+      if (s >= s1 || reach(s, c)) return;
+    }
+  };
+  auto issue = [&](int s, int c, int b) {  // warp 0
+    const int r0 = c * CH, nr = min(ny - r0, CH);
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect(&bar[b], (unsigned)(nr * nx * sizeof(float)));
+    }
+    __syncwarp();
+    fence_proxy_async();
+    for (int y = lane; y < nr; y += 32)
+      bulk_copy(&bar[b], Sb[b] + (size_t)y * nx, T + (((size_t)s * ny + r0 + y) * nz + z) * nx,
+                (unsigned)(nx * sizeof(float)));
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+  }
+  __syncthreads();
+  int s = s0, c = -1;
+  if (s < s1) next(s, c);
+  if (warp == 0 && s < s1) issue(s, c, 0);
+  unsigned phase[2] = {0u, 0u};
+  int b = 0;
+  while (s < s1) {
+    if (__syncthreads_or(!mbar_wait(&bar[b], phase[b]))) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        mbar_wait(&bar[b], phase[b]);
+      }
+      return;
+    }
+    phase[b] ^= 1u;
+    int sn = s, cn = c;
+    next(sn, cn);
+    if (warp == 0 && sn < s1) issue(sn, cn, b ^ 1);
+    const float4 r = rot[vidx[s]];
+    const RotPos R{r.x, r.y, c0};
+    const int r0 = c * CH, nr = min(ny - r0, CH);
+    const float* S = Sb[b];
+    for (int cls = 0; cls < 9; ++cls) {
+      const int c1 = cls % 3, c2 = cls / 3;
+      const int o2f = r0 + (c2 - r0 % 3 + 3) % 3;       // first row of the class in the chunk
+      const int nrow = o2f < r0 + nr ? (r0 + nr - 1 - o2f) / 3 + 1 : 0;
+      const int npt = (nx - c1 + 2) / 3;                 // class columns c1, c1+3, ...
+      // (row, column) walk over nrow x npt points in steps of blockDim.x
+      int q = threadIdx.x / npt, m = threadIdx.x - q * npt;
+      const int dq = blockDim.x / npt, dm = blockDim.x - dq * npt;
+      for (; q < nrow;) {
+        const int o2 = o2f + 3 * q, o1 = c1 + 3 * m;
+        const float val = S[(o2 - r0) * nx + o1];
+        float s1f, s2f;
+        R.pos(o1, o2, s1f, s2f);
+        const float f1 = floorf(s1f), f2 = floorf(s2f);
+        const int j1 = (int)f1, j2 = (int)f2;
+        const float t1 = __fsub_rn(s1f, f1), t2 = __fsub_rn(s2f, f2);
+        const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
+        const bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
+        const bool y0 = j2 >= ya && j2 < yb, y1 = j2 + 1 >= ya && j2 + 1 < yb;
+        float* a0 = acc + j1 + (j2 - ya) * nx;
+        if (x0 && y0) a0[0] += __fmul_rn(__fmul_rn(u1, u2), val);
+        if (x1 && y0) a0[1] += __fmul_rn(__fmul_rn(t1, u2), val);
+        if (x0 && y1) a0[nx] += __fmul_rn(__fmul_rn(u1, t2), val);
+        if (x1 && y1) a0[nx + 1] += __fmul_rn(__fmul_rn(t1, t2), val);
+        q += dq;
+        m += dm;
+        if (m >= npt) {
+          m -= npt;
+          ++q;
+        }
+      }
+      __syncthreads();
+    }
+    b ^= 1;
+    s = sn;
+    c = cn;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nel; k += blockDim.x) outp[k] = acc[k];
 }
 
 // k_reduce_image: img = sum_split imgpart[split]; EM: x .*= img ./ asum
