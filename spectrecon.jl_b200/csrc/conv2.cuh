@@ -34,6 +34,7 @@ namespace spect {
 
 constexpr int kConvThreads = 512;
 constexpr int kConvWarps = kConvThreads / 32;
+static_assert(kConvWarps <= kConvWarpsMax, "x-transform scratch sized for kConvWarpsMax warps");
 
 struct ConvGeom {
   int nx, ny, nz;
@@ -367,6 +368,31 @@ template <int RX>
 __device__ __forceinline__ void apply_psf(float2 (&v)[RX], const float* __restrict__ h, const float* __restrict__ hb,
                                           const Lanes& L, int logCX, bool packed_warp, bool col0) {
   const int CX = (RX > 1) ? 32 : (1 << logCX);
+  if constexpr (RX == 8) {
+    // 256-point layout (fftx256_fwd): the partner X[-k] is in the same lane
+    if (packed_warp && col0) {
+      float2 p[8];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) p[r] = v[7 - r];
+      if (L.l == 0) {
+        p[0] = v[0];
+        p[1] = v[3];
+        p[2] = v[2];
+        p[3] = v[1];
+#pragma unroll
+        for (int r = 4; r < 8; ++r) p[r] = v[11 - r];
+      }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const float al = __ldg(h + r * 32), be = __ldg(hb + r * 32);
+        v[r] = make_float2(al * v[r].x + be * p[r].x, al * v[r].y - be * p[r].y);
+      }
+      return;
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < RX; ++k1) v[k1] = cscale(v[k1], __ldg(h + k1 * CX));
+    return;
+  }
   if (packed_warp) {
     // Y' = alpha Y + beta conj(Y(-k)); registers k1 and RX-k1 are partners
     const int src0 = L.gbase + brev_rt((CX - brev_rt(L.l, logCX)) & (CX - 1), logCX);
@@ -421,6 +447,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
     __syncthreads();
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* const xw = TT.xscr ? TT.xscr + warp * kXScr : nullptr;  // x-transform scratch
   const Lanes L = lanes_of(lane, g.logCX);
   const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
   const int JC = (Q + units - 1) / units;
@@ -488,7 +515,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
           float hp[RX];  // PSF spectrum loads issued before the transform
 #pragma unroll
           for (int k1 = 0; k1 < RX; ++k1) hp[k1] = __ldg(Hy + (size_t)cc * Npx + L.l + k1 * CX);
-          fft_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
+          fftx_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l, xw);
           if (j == 0 && warp == 0) {
             apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX, true, cc == 0);
           } else {
@@ -526,7 +553,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
 #pragma unroll
           for (int k1 = 0; k1 < RX; ++k1) v[k1] = ga[k1 * CX];
         }
-        fft_inv<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
+        fftx_inv<RX>(v, L.l, g.logCX, TT, TT.rx + L.l, xw);
         if (active) {
 #pragma unroll
           for (int r = 0; r < RX; ++r)
@@ -549,6 +576,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
   FftTables TT;
   float2* B = conv_setup<RX, RZ>(a, &TT);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* const xw = TT.xscr ? TT.xscr + warp * kXScr : nullptr;  // x-transform scratch
   const Lanes L = lanes_of(lane, g.logCX);
   const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
   const int iters = (Q + units - 1) / units;
@@ -567,7 +595,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
       float2 v[RX];
 #pragma unroll
       for (int r = 0; r < RX; ++r) v[r] = (T.xrd[r] >= 0) ? B[T.xrd[r] + cc] : make_float2(0.f, 0.f);
-      fft_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
+      fftx_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l, xw);
       if (c < Q) {
         float2* o = a.VsOut + ((size_t)slot * Q + c) * Npx + L.l;
 #pragma unroll
@@ -598,6 +626,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
     __syncthreads();
   }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float2* const xw = TT.xscr ? TT.xscr + warp * kXScr : nullptr;  // x-transform scratch
   const Lanes L = lanes_of(lane, g.logCX);
   const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
   const int JC = (Q + units - 1) / units;
@@ -642,7 +671,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
             v[k1] = REGACC ? vs[REGACC ? j : 0][k1] : Vsl[(size_t)cc * Npx + L.l + k1 * CX];
           apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX,
                         j == 0 && warp == 0, cc == 0);
-          fft_inv<RX>(v, L.l, g.logCX, TT, TT.rx + L.l);
+          fftx_inv<RX>(v, L.l, g.logCX, TT, TT.rx + L.l, xw);
           // adjoint of the replicate padding along x
           float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
 #pragma unroll

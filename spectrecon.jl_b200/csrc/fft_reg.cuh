@@ -63,15 +63,67 @@ __device__ __forceinline__ float2 shfl2(float2 v, int src) {
 //                     w = W_{2^(s+1)}^(l mod 2^s); the lower lane sg = +1, w = 1
 //   rx[k1*32 + l]   = W_Npx^(l k1), rz[k1*32 + l] = W_Npz^(l k1)
 //   base            = W_512^m, m < 512 (for the in-register DFTs)
+//   tw32[kb*32 + l]   = W_32^((l & 3) kb)            (256-point x transforms)
+//   xpair[l]          = (baseA, fA, baseB, fB)        (256-point x transforms)
+//   xscr              = per-warp transpose scratch, kXScr float2 per warp
 struct FftTables {
   const float4* cross;
   const float2* rx;
   const float2* rz;
   const float2* base;
+  const float2* tw32;
+  const int4* xpair;
+  float2* xscr;
 };
 
+constexpr int kXScr = 288;        // float2 per warp: 8 rows of 36 (first transpose)
+constexpr int kConvWarpsMax = 16; // warps of the convolution kernels
+
+__host__ __device__ constexpr int fft_x256_bytes(int RX) {
+  return RX == 8 ? 8 * 32 * 8 + 32 * 16 + kConvWarpsMax * kXScr * 8 : 0;
+}
+
 __host__ __device__ constexpr int fft_tables_bytes(int RX, int RZ) {
-  return SPECT_TW_N * 8 + 5 * 32 * 16 + (RX + RZ) * 32 * 8;
+  return SPECT_TW_N * 8 + 5 * 32 * 16 + (RX + RZ) * 32 * 8 + fft_x256_bytes(RX);
+}
+
+// ---- 256-point x transform (R = 8): the 32-point DFT across the lanes is
+// split as 32 = 8 x 4 and done in registers between two shared-memory
+// transposes, instead of five shuffle stages.
+//   forward: lane l, register r holds x[l + 32 r].  8-point DFT over r and
+//   twiddle W_256^(l k1) (as fft_fwd); transpose M[k1][l] (row stride 36) so
+//   that lane 4 k1 + la holds M[k1][la + 4 lb], lb = 0..7; 8-point DFT over
+//   lb, twiddle W_32^(la kb); transpose Z (address xz_addr) so that each lane
+//   holds two (k1, kb) pairs A and B with la = 0..3; 4-point DFTs over la.
+//   Register ka of pair A holds X[k1A + 8 kbA + 64 ka], register 4 + ka that
+//   of pair B.  Pair B is the spectrum partner of pair A: X[-k] of register r
+//   is register 7 - r of the same lane, except on lane 0, whose pairs (0, 0)
+//   and (0, 4) are their own partners: register (4 - r) & 3 for r < 4 and
+//   11 - r for r >= 4.  Both transposes are free of bank conflicts for 8-byte
+//   accesses.
+//   Lane l = 16 h + 4 q + i: pair A = (q, 4 h + i) for q = 1, 2, 3, (0, i) for
+//   q = 0, h = 0 and (4, i) for q = 0, h = 1; pair B = (8 - k1A, 7 - kbA) when
+//   k1A != 0, (0, 8 - kbA) when k1A == 0 < kbA, and (0, 4) for (0, 0).
+__host__ __device__ constexpr int xz_addr(int k1, int kb, int la) { return 4 * (k1 + 8 * kb) + (la ^ (kb & 3)); }
+
+__host__ __device__ inline void x256_pairs(int l, int& k1A, int& kbA, int& k1B, int& kbB) {
+  const int h = l >> 4, q = (l >> 2) & 3, i = l & 3;
+  k1A = q ? q : 4 * h;
+  kbA = q ? 4 * h + i : i;
+  if (k1A != 0) {
+    k1B = 8 - k1A;
+    kbB = 7 - kbA;
+  } else {
+    k1B = 0;
+    kbB = kbA ? 8 - kbA : 4;
+  }
+}
+
+// frequency index held by lane l, register r of a 256-point x transform
+__host__ __device__ inline int x256_freq(int l, int r) {
+  int k1A, kbA, k1B, kbB;
+  x256_pairs(l, k1A, kbA, k1B, kbB);
+  return r < 4 ? k1A + 8 * kbA + 64 * r : k1B + 8 * kbB + 64 * (r - 4);
 }
 
 // builds the tables in shared memory at `smem` (fft_tables_bytes(RX, RZ)
@@ -102,6 +154,25 @@ __device__ __forceinline__ FftTables build_fft_tables(float2* smem, const float2
   T.rx = rx;
   T.rz = rz;
   T.base = base;
+  T.tw32 = nullptr;
+  T.xpair = nullptr;
+  T.xscr = nullptr;
+  if (RX == 8) {
+    float2* tw32 = rz + RZ * 32;
+    int4* xpair = reinterpret_cast<int4*>(tw32 + 8 * 32);
+    for (int k = threadIdx.x; k < 8 * 32; k += blockDim.x) {
+      const int kb = k >> 5, l = k & 31;
+      tw32[k] = tw_global[(((l & 3) * kb) << (SPECT_TW_LOG - 5)) & (SPECT_TW_N - 1)];
+    }
+    for (int l = threadIdx.x; l < 32; l += blockDim.x) {
+      int k1A, kbA, k1B, kbB;
+      x256_pairs(l, k1A, kbA, k1B, kbB);
+      xpair[l] = make_int4(4 * (k1A + 8 * kbA), kbA & 3, 4 * (k1B + 8 * kbB), kbB & 3);
+    }
+    T.tw32 = tw32;
+    T.xpair = xpair;
+    T.xscr = reinterpret_cast<float2*>(xpair + 32);
+  }
   return T;
 }
 
@@ -187,4 +258,95 @@ __device__ __forceinline__ void fft_inv(float2 (&v)[R], int lc, int logC_rt, con
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = cconj(v[r]);
   }
+}
+
+template <int R>
+__device__ __forceinline__ void reg_dft_at(float2 (&v)[8], int o, const float2* __restrict__ base) {
+  float2 t[R];
+#pragma unroll
+  for (int k = 0; k < R; ++k) t[k] = v[o + k];
+  reg_dft<R>(t, base);
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[o + k] = t[k];
+}
+
+// 256-point forward x transform (see the layout above); w = this warp's
+// transpose scratch, rtw = FftTables::rx + lane
+__device__ __forceinline__ void fftx256_fwd(float2 (&v)[8], int lane, const FftTables& T,
+                                            const float2* __restrict__ rtw, float2* w) {
+  reg_dft<8>(v, T.base);
+#pragma unroll
+  for (int k1 = 1; k1 < 8; ++k1) v[k1] = cmul(v[k1], rtw[k1 * 32]);
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < 8; ++k1) w[k1 * 36 + lane] = v[k1];
+  __syncwarp();
+  const int k1 = lane >> 2, la = lane & 3;
+#pragma unroll
+  for (int lb = 0; lb < 8; ++lb) v[lb] = w[k1 * 36 + la + 4 * lb];
+  reg_dft<8>(v, T.base);
+#pragma unroll
+  for (int kb = 1; kb < 8; ++kb) v[kb] = cmul(v[kb], T.tw32[kb * 32 + lane]);
+  __syncwarp();
+#pragma unroll
+  for (int kb = 0; kb < 8; ++kb) w[xz_addr(k1, kb, la)] = v[kb];
+  __syncwarp();
+  const int4 pr = T.xpair[lane];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    v[a] = w[pr.x + (a ^ pr.y)];
+    v[4 + a] = w[pr.z + (a ^ pr.w)];
+  }
+  reg_dft_at<4>(v, 0, T.base);
+  reg_dft_at<4>(v, 4, T.base);
+}
+
+// inverse of fftx256_fwd (unscaled: returns 256 x[l + 32 r] in register r)
+__device__ __forceinline__ void fftx256_inv(float2 (&v)[8], int lane, const FftTables& T,
+                                            const float2* __restrict__ rtw, float2* w) {
+  // conj(IDFT(y)) = DFT(conj(y)): carry the conjugate through the stages
+#pragma unroll
+  for (int r = 0; r < 8; ++r) v[r] = cconj(v[r]);
+  reg_dft_at<4>(v, 0, T.base);
+  reg_dft_at<4>(v, 4, T.base);
+  const int4 pr = T.xpair[lane];
+  __syncwarp();
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    w[pr.x + (a ^ pr.y)] = v[a];
+    w[pr.z + (a ^ pr.w)] = v[4 + a];
+  }
+  __syncwarp();
+  const int k1 = lane >> 2, la = lane & 3;
+#pragma unroll
+  for (int kb = 0; kb < 8; ++kb) v[kb] = w[xz_addr(k1, kb, la)];
+#pragma unroll
+  for (int kb = 1; kb < 8; ++kb) v[kb] = cmul(v[kb], T.tw32[kb * 32 + lane]);
+  reg_dft<8>(v, T.base);
+  __syncwarp();
+#pragma unroll
+  for (int lb = 0; lb < 8; ++lb) w[k1 * 36 + la + 4 * lb] = v[lb];
+  __syncwarp();
+#pragma unroll
+  for (int q = 0; q < 8; ++q) v[q] = w[q * 36 + lane];
+#pragma unroll
+  for (int q = 1; q < 8; ++q) v[q] = cmul(v[q], rtw[q * 32]);
+  reg_dft<8>(v, T.base);
+#pragma unroll
+  for (int r = 0; r < 8; ++r) v[r] = cconj(v[r]);
+}
+
+// x transforms of the convolution kernels: 256 points through shared
+// memory, other lengths by fft_fwd / fft_inv
+template <int R>
+__device__ __forceinline__ void fftx_fwd(float2 (&v)[R], int lc, int logC_rt, const FftTables& T,
+                                         const float2* __restrict__ rtw, float2* w) {
+  if constexpr (R == 8) fftx256_fwd(v, lc, T, rtw, w);
+  else fft_fwd<R>(v, lc, logC_rt, T, rtw);
+}
+template <int R>
+__device__ __forceinline__ void fftx_inv(float2 (&v)[R], int lc, int logC_rt, const FftTables& T,
+                                         const float2* __restrict__ rtw, float2* w) {
+  if constexpr (R == 8) fftx256_inv(v, lc, T, rtw, w);
+  else fft_inv<R>(v, lc, logC_rt, T, rtw);
 }

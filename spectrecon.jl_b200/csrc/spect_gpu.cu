@@ -392,11 +392,12 @@ int configure(spect_plan_s* p) {
                     !(ns && ns[0] == '1');
     // 1: whole slices (accumulator + two slices); 2: bands of output rows
     // (accumulator band + two chunks of kRotBandRows rows)
-    const size_t rsm = 3 * slice * sizeof(float) + 16;
+    const size_t as = (size_t)acc_stride(g.nx);
+    const size_t rsm = (g.ny * as + 2 * slice) * sizeof(float) + 16;
     int nband = 0;
     size_t bsm = 0;
     for (int nb = 2; nb <= g.ny && ok && rsm > p->max_smem; ++nb) {
-      bsm = sizeof(float) * ((size_t)cdiv(g.ny, nb) * g.nx + 2 * (size_t)kRotBandRows * g.nx) + 16;
+      bsm = sizeof(float) * ((size_t)cdiv(g.ny, nb) * as + 2 * (size_t)kRotBandRows * g.nx) + 16;
       if (bsm <= p->max_smem) {
         nband = nb;
         break;

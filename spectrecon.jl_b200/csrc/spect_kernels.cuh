@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include "bulk_copy.cuh"
+#include "fft_reg.cuh"
 
 
 namespace spect {
@@ -186,6 +187,96 @@ __global__ void k_reduce_views(const float* __restrict__ part, int nv, int nchun
 }
 
 // ------------------------------------------------------------------------
+// ------------------------------------------------------------------------
+// Transpose of the bilinear sampling for one lattice class (c1, c2) of the
+// rotated-grid rows [r0, r0 + nr): point (o1, o2), o1 = c1 mod 3, o2 = c2
+// mod 3, with value S[(o2 - r0) * nx + o1], adds its four bilinear weights
+// (exactly those of bilinear()) into acc rows [ya, yb) (acc row stride as).
+// Inside a class two footprints are >= 3/sqrt 2 > 2 pixels apart, so no two
+// points of the pass touch the same accumulator: each thread keeps two
+// points in flight and the block synchronises only between passes.
+
+// thread walk over the columns o1 = c1, c1 + 3, ... of one class: npt
+// columns; the block steps (dq rows, dm columns) at a time; this thread
+// starts at (q0, m0).  Computed once per kernel (runtime divisions).
+struct ClassCols {
+  int npt, dq, dm, q0, m0;
+};
+__device__ __forceinline__ ClassCols class_cols(int nx, int c1) {
+  ClassCols w;
+  w.npt = (nx - c1 + 2) / 3;
+  w.dq = blockDim.x / w.npt;
+  w.dm = blockDim.x - w.dq * w.npt;
+  w.q0 = threadIdx.x / w.npt;
+  w.m0 = threadIdx.x - w.q0 * w.npt;
+  return w;
+}
+
+__device__ __forceinline__ void scatter_class(const RotPos& R, const float* S, int nx, int r0, int nr, int c1,
+                                              int c2, const ClassCols& cw, float* acc, int as, int ya, int yb) {
+  const int o2f = r0 + (c2 - r0 % 3 + 3) % 3;
+  const int nrow = o2f < r0 + nr ? (r0 + nr - 1 - o2f) / 3 + 1 : 0;
+  const int npt = cw.npt, dq = cw.dq, dm = cw.dm;
+  int q = cw.q0, m = cw.m0;
+  auto step = [&](int& qq, int& mm) {
+    qq += dq;
+    mm += dm;
+    if (mm >= npt) {
+      mm -= npt;
+      ++qq;
+    }
+  };
+  while (q < nrow) {
+    int qb = q, mb = m;
+    step(qb, mb);
+    const bool hasb = qb < nrow;
+    float w[2][4], val[2], old[2][4];
+    int base[2];
+    bool ok[2][4];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int qq = k ? qb : q, mm = k ? mb : m;
+      const int o2 = o2f + 3 * qq, o1 = c1 + 3 * mm;
+      const bool act = k ? hasb : true;
+      val[k] = act ? S[(o2 - r0) * nx + o1] : 0.f;
+      float s1, s2;
+      R.pos(o1, o2, s1, s2);
+      const float f1 = floorf(s1), f2 = floorf(s2);
+      const int j1 = (int)f1, j2 = (int)f2;
+      const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
+      const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
+      const bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
+      const bool y0 = j2 >= ya && j2 < yb, y1 = j2 + 1 >= ya && j2 + 1 < yb;
+      ok[k][0] = act && x0 && y0;
+      ok[k][1] = act && x1 && y0;
+      ok[k][2] = act && x0 && y1;
+      ok[k][3] = act && x1 && y1;
+      w[k][0] = __fmul_rn(u1, u2);
+      w[k][1] = __fmul_rn(t1, u2);
+      w[k][2] = __fmul_rn(u1, t2);
+      w[k][3] = __fmul_rn(t1, t2);
+      base[k] = j1 + (j2 - ya) * as;
+    }
+    const int off[4] = {0, 1, 0, 1};
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int t = 0; t < 4; ++t) old[k][t] = ok[k][t] ? acc[base[k] + off[t] + (t >> 1) * as] : 0.f;
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (ok[k][t]) acc[base[k] + off[t] + (t >> 1) * as] = __fadd_rn(old[k][t], __fmul_rn(w[k][t], val[k]));
+    q = qb;
+    m = mb;
+    step(q, m);
+  }
+}
+
+// accumulator row stride: nx padded to 5 mod 32 so that the taps of a warp's
+// points along a rotated line spread over the banks
+__host__ __device__ constexpr int acc_stride(int nx) { return nx + ((5 - nx) % 32 + 32) % 32; }
+
 // k_rot_adj: grid (nz, nsplit), block kRotAdjThreads.  Accumulates
 // sum_s R'(a_s .* T_s) for the slots of this split into acc (shared or the
 // global per-CTA buffer) and adds/writes it into imgpart[split][z][:][:].
@@ -226,16 +317,21 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
     segsum = S + slice;
   }
   float* outp = imgpart + ((size_t)split * nz + z) * slice;
-  for (int k = threadIdx.x; k < slice; k += blockDim.x) acc[k] = accumulate ? outp[k] : 0.f;
+  // STAGE pads the accumulator rows (acc_stride); the other paths keep nx
+  const int as = STAGE ? acc_stride(nx) : nx;
+  const ClassCols cw0 = class_cols(nx, 0), cw1 = class_cols(nx, 1), cw2 = class_cols(nx, 2);
+  for (int k = threadIdx.x; k < slice; k += blockDim.x) acc[k + (k / nx) * (as - nx)] = accumulate ? outp[k] : 0.f;
   const float* mu = mumap + (size_t)z * slice;
   const int per = (nv + gridDim.y - 1) / gridDim.y;
   const int s0 = split * per, s1 = min(nv, s0 + per);
   const float mdy = -g.dy;
   const int seglen = (ny + nseg - 1) / nseg;
   const int myseg = threadIdx.x / nx, o1s = threadIdx.x - myseg * nx;
-  float* Sb[2] = {S, S + slice};
+  if (STAGE) S = acc + (size_t)ny * as;
+  float* const Sb0 = S;
+  float* const Sb1 = S + slice;
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(S + 2 * slice);
-  unsigned phase[2] = {0u, 0u};
+  unsigned phases = 0u;  // bit b: parity of buffer b's next phase
   // warp 0: rows y of slot sl's slice z into buffer b
   auto issue = [&](int sl, int b) {
     if (lane == 0) {
@@ -244,8 +340,9 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
     }
     __syncwarp();
     fence_proxy_async();
+    float* dst = b ? Sb1 : Sb0;
     for (int y = lane; y < ny; y += 32)
-      bulk_copy(&bar[b], Sb[b] + (size_t)y * nx, T + (((size_t)sl * ny + y) * nz + z) * nx,
+      bulk_copy(&bar[b], dst + (size_t)y * nx, T + (((size_t)sl * ny + y) * nz + z) * nx,
                 (unsigned)(nx * sizeof(float)));
   };
   if (STAGE) {
@@ -265,15 +362,16 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
     if (STAGE) {
       // this slot's rows have landed; the block barrier also ends the
       // previous slot's scatter, so the other buffer is free
-      if (__syncthreads_or(!mbar_wait(&bar[b], phase[b]))) {
+      const unsigned par = (phases >> b) & 1u;
+      if (__syncthreads_or(!mbar_wait(&bar[b], par))) {
         if (threadIdx.x == 0) {
           atomicExch(err, 1);
-          mbar_wait(&bar[b], phase[b]);
+          mbar_wait(&bar[b], par);
         }
         return;
       }
-      phase[b] ^= 1u;
-      S = Sb[b];
+      phases ^= 1u << b;
+      S = b ? Sb1 : Sb0;
       if (warp == 0 && s + 1 < s1) issue(s + 1, b ^ 1);
     } else {
       __syncthreads();
@@ -320,30 +418,16 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
     //    o2 mod 3); inside a class the 2x2 footprints of two points are >= 2.1
     //    pixels apart (|Rot (3a,3b)|_inf >= 3/sqrt 2), so they never overlap
     for (int cls = 0; cls < 9; ++cls) {
-      const int c1 = cls % 3, c2 = cls / 3;
-      for (int o2 = c2 + 3 * warp; o2 < ny; o2 += 3 * nwarps) {
-        for (int o1 = c1 + 3 * lane; o1 < nx; o1 += 96) {
-          const float val = S[o1 + o2 * nx];
-          float s1, s2;
-          R.pos(o1, o2, s1, s2);
-          const float f1 = floorf(s1), f2 = floorf(s2);
-          const int j1 = (int)f1, j2 = (int)f2;
-          const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
-          const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
-          const bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
-          const bool y0 = (unsigned)j2 < (unsigned)ny, y1 = (unsigned)(j2 + 1) < (unsigned)ny;
-          float* a0 = acc + j1 + j2 * nx;
-          if (x0 && y0) a0[0] += __fmul_rn(__fmul_rn(u1, u2), val);
-          if (x1 && y0) a0[1] += __fmul_rn(__fmul_rn(t1, u2), val);
-          if (x0 && y1) a0[nx] += __fmul_rn(__fmul_rn(u1, t2), val);
-          if (x1 && y1) a0[nx + 1] += __fmul_rn(__fmul_rn(t1, t2), val);
-        }
-      }
+      const int c1 = cls % 3;
+      scatter_class(R, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, 0, ny);
       __syncthreads();
     }
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < slice; k += blockDim.x) outp[k] = acc[k];
+  for (int k = threadIdx.x; k < slice; k += blockDim.x) {
+    const int y = k / nx;
+    outp[k] = acc[k + y * (as - nx)];
+  }
 }
 
 // k_rot_adj_band: the adjoint rotation for slices too large for shared
@@ -368,13 +452,16 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
   if (ya >= yb) return;  // uniform over the block
   constexpr int CH = kRotBandRows;
   const int nch = (ny + CH - 1) / CH;
+  const int as = acc_stride(nx);
+  const ClassCols cw0 = class_cols(nx, 0), cw1 = class_cols(nx, 1), cw2 = class_cols(nx, 2);
   float* acc = reinterpret_cast<float*>(smem4);
-  float* Sb[2] = {acc + (size_t)rows * nx, acc + (size_t)rows * nx + (size_t)CH * nx};
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(Sb[1] + (size_t)CH * nx);
+  float* const Sb0 = acc + (size_t)rows * as;
+  float* const Sb1 = Sb0 + (size_t)CH * nx;
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(Sb1 + (size_t)CH * nx);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* outp = imgpart + (((size_t)split * nz + z) * ny + ya) * nx;
   const int nel = (yb - ya) * nx;
-  for (int k = threadIdx.x; k < nel; k += blockDim.x) acc[k] = accumulate ? outp[k] : 0.f;
+  for (int k = threadIdx.x; k < nel; k += blockDim.x) acc[k + (k / nx) * (as - nx)] = accumulate ? outp[k] : 0.f;
   const int per = (nv + gridDim.y - 1) / gridDim.y;
   const int s0 = split * per, s1 = min(nv, s0 + per);
   const float c0 = g.c0;
@@ -405,8 +492,9 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
     }
     __syncwarp();
     fence_proxy_async();
+    float* dst = b ? Sb1 : Sb0;
     for (int y = lane; y < nr; y += 32)
-      bulk_copy(&bar[b], Sb[b] + (size_t)y * nx, T + (((size_t)s * ny + r0 + y) * nz + z) * nx,
+      bulk_copy(&bar[b], dst + (size_t)y * nx, T + (((size_t)s * ny + r0 + y) * nz + z) * nx,
                 (unsigned)(nx * sizeof(float)));
   };
   if (threadIdx.x == 0) {
@@ -417,55 +505,28 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
   int s = s0, c = -1;
   if (s < s1) next(s, c);
   if (warp == 0 && s < s1) issue(s, c, 0);
-  unsigned phase[2] = {0u, 0u};
+  unsigned phases = 0u;  // bit b: parity of buffer b's next phase
   int b = 0;
   while (s < s1) {
-    if (__syncthreads_or(!mbar_wait(&bar[b], phase[b]))) {
+    const unsigned par = (phases >> b) & 1u;
+    if (__syncthreads_or(!mbar_wait(&bar[b], par))) {
       if (threadIdx.x == 0) {
         atomicExch(err, 1);
-        mbar_wait(&bar[b], phase[b]);
+        mbar_wait(&bar[b], par);
       }
       return;
     }
-    phase[b] ^= 1u;
+    phases ^= 1u << b;
     int sn = s, cn = c;
     next(sn, cn);
     if (warp == 0 && sn < s1) issue(sn, cn, b ^ 1);
     const float4 r = rot[vidx[s]];
     const RotPos R{r.x, r.y, c0};
     const int r0 = c * CH, nr = min(ny - r0, CH);
-    const float* S = Sb[b];
+    const float* S = b ? Sb1 : Sb0;
     for (int cls = 0; cls < 9; ++cls) {
-      const int c1 = cls % 3, c2 = cls / 3;
-      const int o2f = r0 + (c2 - r0 % 3 + 3) % 3;       // first row of the class in the chunk
-      const int nrow = o2f < r0 + nr ? (r0 + nr - 1 - o2f) / 3 + 1 : 0;
-      const int npt = (nx - c1 + 2) / 3;                 // class columns c1, c1+3, ...
-      // (row, column) walk over nrow x npt points in steps of blockDim.x
-      int q = threadIdx.x / npt, m = threadIdx.x - q * npt;
-      const int dq = blockDim.x / npt, dm = blockDim.x - dq * npt;
-      for (; q < nrow;) {
-        const int o2 = o2f + 3 * q, o1 = c1 + 3 * m;
-        const float val = S[(o2 - r0) * nx + o1];
-        float s1f, s2f;
-        R.pos(o1, o2, s1f, s2f);
-        const float f1 = floorf(s1f), f2 = floorf(s2f);
-        const int j1 = (int)f1, j2 = (int)f2;
-        const float t1 = __fsub_rn(s1f, f1), t2 = __fsub_rn(s2f, f2);
-        const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
-        const bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
-        const bool y0 = j2 >= ya && j2 < yb, y1 = j2 + 1 >= ya && j2 + 1 < yb;
-        float* a0 = acc + j1 + (j2 - ya) * nx;
-        if (x0 && y0) a0[0] += __fmul_rn(__fmul_rn(u1, u2), val);
-        if (x1 && y0) a0[1] += __fmul_rn(__fmul_rn(t1, u2), val);
-        if (x0 && y1) a0[nx] += __fmul_rn(__fmul_rn(u1, t2), val);
-        if (x1 && y1) a0[nx + 1] += __fmul_rn(__fmul_rn(t1, t2), val);
-        q += dq;
-        m += dm;
-        if (m >= npt) {
-          m -= npt;
-          ++q;
-        }
-      }
+      const int c1 = cls % 3;
+      scatter_class(R, S, nx, r0, nr, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, ya, yb);
       __syncthreads();
     }
     b ^= 1;
@@ -473,7 +534,7 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
     c = cn;
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < nel; k += blockDim.x) outp[k] = acc[k];
+  for (int k = threadIdx.x; k < nel; k += blockDim.x) outp[k] = acc[k + (k / nx) * (as - nx)];
 }
 
 // k_reduce_image: img = sum_split imgpart[split]; EM: x .*= img ./ asum
@@ -551,7 +612,9 @@ __global__ void k_psf_permute(const float* __restrict__ H, int nplanes, int Npx,
     const int c = (int)(r % (Q + 1));
     const size_t pl = r / (Q + 1);
     const int k1 = pos / CX, l = pos - k1 * CX;
-    const int kx = k1 + RX * (logCX ? (int)(__brev(l) >> (32 - logCX)) : 0);
+    // lane l, register k1 of the x transform: the 256-point layout of
+    // fftx256_fwd, else X[k1 + RX brev(l)]
+    const int kx = RX == 8 ? x256_freq(l, k1) : k1 + RX * (logCX ? (int)(__brev(l) >> (32 - logCX)) : 0);
     const float* Hp = H + pl * Hz * Npx;
     float v;
     if (c == 0 || c == Q) {
