@@ -374,8 +374,8 @@ int configure(spect_plan_s* p) {
                           ? std::max(p->nsplit_adj, 16)
                           : p->nsplit_adj;
   if (p->rota_smem_ok) {
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
-    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
+    CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->max_smem));
   } else {
     size_t per = 2 * slice + (size_t)nseg * g.nx;
     STATUS_TRY(dalloc(p, &p->d_gscr_adj, per * g.nz * p->nsplit_adj_max));
@@ -392,12 +392,12 @@ int configure(spect_plan_s* p) {
                     !(ns && ns[0] == '1');
     // 1: whole slices (accumulator + two slices); 2: bands of output rows
     // (accumulator band + two chunks of kRotBandRows rows)
-    const size_t as = (size_t)acc_stride(g.nx);
-    const size_t rsm = (g.ny * as + 2 * slice) * sizeof(float) + 16;
+    const int as = acc_stride(g.nx);
+    const size_t rsm = ((size_t)acc_floats(g.ny, as) + 2 * slice) * sizeof(float) + 16;
     int nband = 0;
     size_t bsm = 0;
     for (int nb = 2; nb <= g.ny && ok && rsm > p->max_smem; ++nb) {
-      bsm = sizeof(float) * ((size_t)cdiv(g.ny, nb) * as + 2 * (size_t)kRotBandRows * g.nx) + 16;
+      bsm = sizeof(float) * ((size_t)acc_floats(cdiv(g.ny, nb), as) + 2 * (size_t)kRotBandRows * g.nx) + 16;
       if (bsm <= p->max_smem) {
         nband = nb;
         break;
@@ -408,7 +408,7 @@ int configure(spect_plan_s* p) {
     p->conv_smem_adj = p->adj_stage ? cadj : p->conv_smem;
     p->rota_smem_stage = p->adj_stage == 1 ? rsm : bsm;
     if (p->adj_stage == 1)
-      CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj_stream, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)p->max_smem));
     if (p->adj_stage == 2)
       CUDA_TRY(cudaFuncSetAttribute((const void*)k_rot_adj_band, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -581,15 +581,15 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
            if (p->adj_stage == 2) k_rot_adj_band<<<dim3(g.nz, nsplit, p->rot_nband), kRotAdjThreads,
                                                    p->rota_smem_stage, st>>>(
                g, p->d_P, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rot_nband, p->d_err);
-           else if (p->adj_stage == 1) k_rot_adj<true, true><<<grid, kRotAdjThreads, p->rota_smem_stage, st>>>(
-               g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, 1, p->d_gscr_adj,
-               p->d_err);
-           else if (p->d_att) k_rot_adj<true, false><<<grid, kRotAdjThreads, rsm, st>>>(
+           else if (p->adj_stage == 1) k_rot_adj_stream<<<std::min(g.nz * nsplit, p->sm_count), kRotAdjThreads,
+                                                           p->rota_smem_stage, st>>>(
+               g, p->d_P, p->d_rot, vi, nv, nsplit, p->d_imgpart, g0 > 0 ? 1 : 0, p->d_err);
+           else if (p->d_att) k_rot_adj<true><<<grid, kRotAdjThreads, rsm, st>>>(
                g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
-               p->d_gscr_adj, p->d_err);
-           else k_rot_adj<false, false><<<grid, kRotAdjThreads, rsm, st>>>(
+               p->d_gscr_adj);
+           else k_rot_adj<false><<<grid, kRotAdjThreads, rsm, st>>>(
                g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
-               p->d_gscr_adj, p->d_err));
+               p->d_gscr_adj));
   }
   int rb = (int)std::min<size_t>((p->N + 255) / 256, (size_t)p->sm_count * 16);
   LAUNCH(p, K_REDUCE_IMAGE, st, "k_reduce_image",

@@ -191,7 +191,9 @@ __global__ void k_reduce_views(const float* __restrict__ part, int nv, int nchun
 // Transpose of the bilinear sampling for one lattice class (c1, c2) of the
 // rotated-grid rows [r0, r0 + nr): point (o1, o2), o1 = c1 mod 3, o2 = c2
 // mod 3, with value S[(o2 - r0) * nx + o1], adds its four bilinear weights
-// (exactly those of bilinear()) into acc rows [ya, yb) (acc row stride as).
+// (exactly those of bilinear()) into acc rows [ya, yb) (acc row stride as
+// >= nx + 2).  acc must be guarded: rows ya-1 and yb and columns -1 and nx
+// addressable (the padding of the neighbouring rows serves as columns).
 // Inside a class two footprints are >= 3/sqrt 2 > 2 pixels apart, so no two
 // points of the pass touch the same accumulator: each thread keeps two
 // points in flight and the block synchronises only between passes.
@@ -212,6 +214,7 @@ __device__ __forceinline__ ClassCols class_cols(int nx, int c1) {
   return w;
 }
 
+template <bool GUARD>
 __device__ __forceinline__ void scatter_class(const RotPos& R, const float* S, int nx, int r0, int nr, int c1,
                                               int c2, const ClassCols& cw, float* acc, int as, int ya, int yb) {
   const int o2f = r0 + (c2 - r0 % 3 + 3) % 3;
@@ -232,7 +235,7 @@ __device__ __forceinline__ void scatter_class(const RotPos& R, const float* S, i
     const bool hasb = qb < nrow;
     float w[2][4], val[2], old[2][4];
     int base[2];
-    bool ok[2][4];
+    bool ok[2], tk[2][4];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       const int qq = k ? qb : q, mm = k ? mb : m;
@@ -245,12 +248,17 @@ __device__ __forceinline__ void scatter_class(const RotPos& R, const float* S, i
       const int j1 = (int)f1, j2 = (int)f2;
       const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
       const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
-      const bool x0 = (unsigned)j1 < (unsigned)nx, x1 = (unsigned)(j1 + 1) < (unsigned)nx;
-      const bool y0 = j2 >= ya && j2 < yb, y1 = j2 + 1 >= ya && j2 + 1 < yb;
-      ok[k][0] = act && x0 && y0;
-      ok[k][1] = act && x1 && y0;
-      ok[k][2] = act && x0 && y1;
-      ok[k][3] = act && x1 && y1;
+      // GUARD: footprint {j1, j1+1} x {j2, j2+1} inside the guarded
+      // accumulator (columns -1..nx, rows ya-1..yb); taps outside the image
+      // land in guard cells, which are never read back.  Otherwise each tap
+      // is checked against the image.
+      ok[k] = act && (unsigned)(j1 + 1) <= (unsigned)nx && (unsigned)(j2 + 1 - ya) <= (unsigned)(yb - ya);
+      if (!GUARD) {
+        tk[k][0] = j1 >= 0 && j2 >= ya;
+        tk[k][1] = j1 + 1 < nx && j2 >= ya;
+        tk[k][2] = j1 >= 0 && j2 + 1 < yb;
+        tk[k][3] = j1 + 1 < nx && j2 + 1 < yb;
+      }
       w[k][0] = __fmul_rn(u1, u2);
       w[k][1] = __fmul_rn(t1, u2);
       w[k][2] = __fmul_rn(u1, t2);
@@ -260,22 +268,32 @@ __device__ __forceinline__ void scatter_class(const RotPos& R, const float* S, i
     const int off[4] = {0, 1, 0, 1};
 #pragma unroll
     for (int k = 0; k < 2; ++k)
+      if (ok[k]) {
 #pragma unroll
-      for (int t = 0; t < 4; ++t) old[k][t] = ok[k][t] ? acc[base[k] + off[t] + (t >> 1) * as] : 0.f;
+        for (int t = 0; t < 4; ++t)
+          old[k][t] = (GUARD || tk[k][t]) ? acc[base[k] + off[t] + (t >> 1) * as] : 0.f;
+      }
 #pragma unroll
     for (int k = 0; k < 2; ++k)
+      if (ok[k]) {
 #pragma unroll
-      for (int t = 0; t < 4; ++t)
-        if (ok[k][t]) acc[base[k] + off[t] + (t >> 1) * as] = __fadd_rn(old[k][t], __fmul_rn(w[k][t], val[k]));
+        for (int t = 0; t < 4; ++t)
+          if (GUARD || tk[k][t])
+            acc[base[k] + off[t] + (t >> 1) * as] = __fadd_rn(old[k][t], __fmul_rn(w[k][t], val[k]));
+      }
     q = qb;
     m = mb;
     step(q, m);
   }
 }
 
-// accumulator row stride: nx padded to 5 mod 32 so that the taps of a warp's
-// points along a rotated line spread over the banks
-__host__ __device__ constexpr int acc_stride(int nx) { return nx + ((5 - nx) % 32 + 32) % 32; }
+// guarded accumulator row stride: at least nx + 2 (the padding of a row
+// holds guard columns nx and -1 of the next row), 5 mod 32 so that the taps
+// of a warp's points along a rotated line spread over the banks
+__host__ __device__ constexpr int acc_stride(int nx) { return nx + 2 + ((5 - (nx + 2)) % 32 + 32) % 32; }
+// floats of a guarded accumulator of `rows` rows (guard rows above and
+// below), rounded to 16 bytes; its element (0, 0) is at offset as + 1
+__host__ __device__ constexpr int acc_floats(int rows, int as) { return ((rows + 2) * as + 3) & ~3; }
 
 // k_rot_adj: grid (nz, nsplit), block kRotAdjThreads.  Accumulates
 // sum_s R'(a_s .* T_s) for the slots of this split into acc (shared or the
@@ -283,20 +301,16 @@ __host__ __device__ constexpr int acc_stride(int nx) { return nx + ((5 - nx) % 3
 // CACHED: a_s from the attenuation cache; otherwise rotated mu-map + depth
 // scan per view (imrotate! of the mu-map and the attenuation of
 // src/backproject.jl:285-317).
-// STAGE (with CACHED): T already carries a_s (the adjoint convolution
-// multiplied it in); each slot's slice rows are bulk-copied into one of two
-// shared buffers while the previous slot is scattered.  Shared memory:
-// acc, two slices, two mbarriers.
 constexpr int kRotAdjThreads = 512;
 
-template <bool CACHED, bool STAGE>
+template <bool CACHED>
 __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const float* __restrict__ T,
                                                                 const float* __restrict__ mumap,
                                                                 const float* __restrict__ att,
                                                                 const float4* __restrict__ rot,
                                                                 const int* __restrict__ vidx, int nv,
                                                                 float* __restrict__ imgpart, int accumulate,
-                                                                int use_smem, float* __restrict__ gscr, int* err) {
+                                                                int use_smem, float* __restrict__ gscr) {
   extern __shared__ float4 smem4[];
   const int nx = g.nx, ny = g.ny, nz = g.nz;
   const int z = blockIdx.x, split = blockIdx.y;
@@ -317,67 +331,22 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
     segsum = S + slice;
   }
   float* outp = imgpart + ((size_t)split * nz + z) * slice;
-  // STAGE pads the accumulator rows (acc_stride); the other paths keep nx
-  const int as = STAGE ? acc_stride(nx) : nx;
   const ClassCols cw0 = class_cols(nx, 0), cw1 = class_cols(nx, 1), cw2 = class_cols(nx, 2);
-  for (int k = threadIdx.x; k < slice; k += blockDim.x) acc[k + (k / nx) * (as - nx)] = accumulate ? outp[k] : 0.f;
+  for (int y = warp; y < ny; y += nwarps)
+    for (int x = lane; x < nx; x += 32) acc[y * nx + x] = accumulate ? outp[y * nx + x] : 0.f;
   const float* mu = mumap + (size_t)z * slice;
   const int per = (nv + gridDim.y - 1) / gridDim.y;
   const int s0 = split * per, s1 = min(nv, s0 + per);
   const float mdy = -g.dy;
   const int seglen = (ny + nseg - 1) / nseg;
   const int myseg = threadIdx.x / nx, o1s = threadIdx.x - myseg * nx;
-  if (STAGE) S = acc + (size_t)ny * as;
-  float* const Sb0 = S;
-  float* const Sb1 = S + slice;
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(S + 2 * slice);
-  unsigned phases = 0u;  // bit b: parity of buffer b's next phase
-  // warp 0: rows y of slot sl's slice z into buffer b
-  auto issue = [&](int sl, int b) {
-    if (lane == 0) {
-      fence_proxy_async();
-      mbar_expect(&bar[b], (unsigned)(slice * sizeof(float)));
-    }
-    __syncwarp();
-    fence_proxy_async();
-    float* dst = b ? Sb1 : Sb0;
-    for (int y = lane; y < ny; y += 32)
-      bulk_copy(&bar[b], dst + (size_t)y * nx, T + (((size_t)sl * ny + y) * nz + z) * nx,
-                (unsigned)(nx * sizeof(float)));
-  };
-  if (STAGE) {
-    if (threadIdx.x == 0) {
-      mbar_init(&bar[0]);
-      mbar_init(&bar[1]);
-    }
-    __syncthreads();
-    if (warp == 0 && s0 < s1) issue(s0, 0);
-  }
   for (int s = s0; s < s1; ++s) {
     const int v = vidx[s];
     const float4 r = rot[v];
     RotPos R{r.x, r.y, g.c0};
     const bool ident = r.z != 0.f;
-    const int b = (s - s0) & 1;
-    if (STAGE) {
-      // this slot's rows have landed; the block barrier also ends the
-      // previous slot's scatter, so the other buffer is free
-      const unsigned par = (phases >> b) & 1u;
-      if (__syncthreads_or(!mbar_wait(&bar[b], par))) {
-        if (threadIdx.x == 0) {
-          atomicExch(err, 1);
-          mbar_wait(&bar[b], par);
-        }
-        return;
-      }
-      phases ^= 1u << b;
-      S = b ? Sb1 : Sb0;
-      if (warp == 0 && s + 1 < s1) issue(s + 1, b ^ 1);
-    } else {
-      __syncthreads();
-    }
-    if (STAGE) {
-    } else if (CACHED) {
+    __syncthreads();
+    if (CACHED) {
       // S = a .* T on the rotated grid (coalesced rows of x)
       const float* av = att + ((size_t)v * ny * nz + z) * nx;
       const float* tv = T + ((size_t)s * ny * nz + z) * nx;
@@ -419,14 +388,118 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
     //    pixels apart (|Rot (3a,3b)|_inf >= 3/sqrt 2), so they never overlap
     for (int cls = 0; cls < 9; ++cls) {
       const int c1 = cls % 3;
-      scatter_class(R, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, 0, ny);
+      scatter_class<false>(R, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, nx, 0, ny);
       __syncthreads();
     }
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < slice; k += blockDim.x) {
-    const int y = k / nx;
-    outp[k] = acc[k + y * (as - nx)];
+  for (int y = warp; y < ny; y += nwarps)
+    for (int x = lane; x < nx; x += 32) outp[y * nx + x] = acc[y * nx + x];
+}
+
+// k_rot_adj_stream: persistent form of the cached adjoint rotation for
+// premultiplied slices (the adjoint convolution applied a_s).  Work items are
+// (slice z, view split) pairs, item = split * nz + z, taken by the blocks in
+// grid-stride order; each block walks the sequence of (item, slot) of its
+// items and bulk-copies the rows of the next slot's slice (which may belong
+// to its next item) into the second of two shared buffers while it scatters
+// the current one, so only the block's very first copy is waited on.  The
+// accumulator (rows padded to acc_stride) is written to imgpart[split][z] at
+// the end of each item and re-initialised for the next.
+__global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_stream(Geom g, const float* __restrict__ T,
+                                                                       const float4* __restrict__ rot,
+                                                                       const int* __restrict__ vidx, int nv,
+                                                                       int nsplit, float* __restrict__ imgpart,
+                                                                       int accumulate, int* err) {
+  extern __shared__ float4 smem4[];
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int slice = nx * ny;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int as = acc_stride(nx);
+  const ClassCols cw0 = class_cols(nx, 0), cw1 = class_cols(nx, 1), cw2 = class_cols(nx, 2);
+  float* const acc = reinterpret_cast<float*>(smem4) + as + 1;  // guarded (acc_floats)
+  float* const Sb0 = reinterpret_cast<float*>(smem4) + acc_floats(ny, as);
+  float* const Sb1 = Sb0 + slice;
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(Sb1 + slice);
+  const int nitems = nz * nsplit;
+  const int per = (nv + nsplit - 1) / nsplit;
+  // next (item, slot) of this block after (it, s); it >= nitems when done
+  auto next = [&](int& it, int& s) {
+    if (s + 1 < min(nv, (it / nz) * per + per)) {
+      ++s;
+      return;
+    }
+    for (it += gridDim.x; it < nitems; it += gridDim.x) {
+      s = (it / nz) * per;
+      if (s < nv) return;
+    }
+  };
+  auto issue = [&](int it, int sl, int b) {  // warp 0
+    const int z = it % nz;
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect(&bar[b], (unsigned)(slice * sizeof(float)));
+    }
+    __syncwarp();
+    fence_proxy_async();
+    float* dst = b ? Sb1 : Sb0;
+    for (int y = lane; y < ny; y += 32)
+      bulk_copy(&bar[b], dst + (size_t)y * nx, T + (((size_t)sl * ny + y) * nz + z) * nx,
+                (unsigned)(nx * sizeof(float)));
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0]);
+    mbar_init(&bar[1]);
+  }
+  // splits without slots still own a partial image: zero it on a first group
+  if (!accumulate)
+    for (int e = blockIdx.x; e < nitems; e += gridDim.x)
+      if ((e / nz) * per >= nv) {
+        float* o = imgpart + ((size_t)(e / nz) * nz + e % nz) * slice;
+        for (int k = threadIdx.x; k < slice; k += blockDim.x) o[k] = 0.f;
+      }
+  __syncthreads();
+  int it = blockIdx.x - (int)gridDim.x, s = nv;  // advance to the first (item, slot)
+  next(it, s);
+  if (warp == 0 && it < nitems) issue(it, s, 0);
+  unsigned phases = 0u;  // bit b: parity of buffer b's next phase
+  int b = 0, cur = -1;
+  while (it < nitems) {
+    const int z = it % nz, split = it / nz;
+    float* outp = imgpart + ((size_t)split * nz + z) * slice;
+    if (it != cur) {
+      // same (y, x) mapping as the write-out below: no barrier needed
+      for (int y = warp; y < ny; y += nwarps)
+        for (int x = lane; x < nx; x += 32) acc[y * as + x] = accumulate ? outp[y * nx + x] : 0.f;
+      cur = it;
+    }
+    const unsigned par = (phases >> b) & 1u;
+    if (__syncthreads_or(!mbar_wait(&bar[b], par))) {
+      if (threadIdx.x == 0) {
+        atomicExch(err, 1);
+        mbar_wait(&bar[b], par);
+      }
+      return;
+    }
+    phases ^= 1u << b;
+    int it2 = it, s2 = s;
+    next(it2, s2);
+    if (warp == 0 && it2 < nitems) issue(it2, s2, b ^ 1);
+    const float4 r = rot[vidx[s]];
+    const RotPos R{r.x, r.y, g.c0};
+    const float* S = b ? Sb1 : Sb0;
+    for (int cls = 0; cls < 9; ++cls) {
+      const int c1 = cls % 3;
+      scatter_class<true>(R, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, 0, ny);
+      __syncthreads();
+    }
+    if (it2 != it) {
+      for (int y = warp; y < ny; y += nwarps)
+        for (int x = lane; x < nx; x += 32) outp[y * nx + x] = acc[y * as + x];
+    }
+    b ^= 1;
+    it = it2;
+    s = s2;
   }
 }
 
@@ -454,14 +527,15 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
   const int nch = (ny + CH - 1) / CH;
   const int as = acc_stride(nx);
   const ClassCols cw0 = class_cols(nx, 0), cw1 = class_cols(nx, 1), cw2 = class_cols(nx, 2);
-  float* acc = reinterpret_cast<float*>(smem4);
-  float* const Sb0 = acc + (size_t)rows * as;
+  float* const acc = reinterpret_cast<float*>(smem4) + as + 1;  // guarded (acc_floats)
+  float* const Sb0 = reinterpret_cast<float*>(smem4) + acc_floats(rows, as);
   float* const Sb1 = Sb0 + (size_t)CH * nx;
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(Sb1 + (size_t)CH * nx);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* outp = imgpart + (((size_t)split * nz + z) * ny + ya) * nx;
-  const int nel = (yb - ya) * nx;
-  for (int k = threadIdx.x; k < nel; k += blockDim.x) acc[k + (k / nx) * (as - nx)] = accumulate ? outp[k] : 0.f;
+  const int nwarps = blockDim.x >> 5;
+  for (int y = warp; y < yb - ya; y += nwarps)
+    for (int x = lane; x < nx; x += 32) acc[y * as + x] = accumulate ? outp[y * nx + x] : 0.f;
   const int per = (nv + gridDim.y - 1) / gridDim.y;
   const int s0 = split * per, s1 = min(nv, s0 + per);
   const float c0 = g.c0;
@@ -526,7 +600,7 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
     const float* S = b ? Sb1 : Sb0;
     for (int cls = 0; cls < 9; ++cls) {
       const int c1 = cls % 3;
-      scatter_class(R, S, nx, r0, nr, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, ya, yb);
+      scatter_class<true>(R, S, nx, r0, nr, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, ya, yb);
       __syncthreads();
     }
     b ^= 1;
@@ -534,7 +608,8 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
     c = cn;
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < nel; k += blockDim.x) outp[k] = acc[k + (k / nx) * (as - nx)];
+  for (int y = warp; y < yb - ya; y += nwarps)
+    for (int x = lane; x < nx; x += 32) outp[y * nx + x] = acc[y * as + x];
 }
 
 // k_reduce_image: img = sum_split imgpart[split]; EM: x .*= img ./ asum
