@@ -78,14 +78,92 @@ __device__ __forceinline__ Lanes lanes_of(int lane, int logC) {
   return L;
 }
 
-// shared memory: [FFT tables (fft_tables_bytes(RX, RZ))][B when bsmem]
+// Per-lane tables of the inverse z transform of a row pair (one entry per
+// register k1 and lane, [k1 * 32 + lane]):
+//   zgc  gather of the Hermitian spectrum from the stored columns: column c
+//        and multipliers (mx, my, sy): a = (mx a.x + my a.y, sy a.y) turns the
+//        stored value into the input of fft_inv (sy = -1: conjugate partner;
+//        (1,0,0) / (0,1,0): the real DC / Nyquist packed in column 0)
+//   zst  output sample z of register r: (z, or -1 outside the image; flags
+//        1: z in the low fold range, 2: high fold range, 4: z == 0,
+//        8: z == nz - 1)
+struct ZTabs {
+  const float4* zgc;
+  const int2* zst;
+};
+
+template <int RZ>
+__host__ __device__ constexpr int ztabs_bytes() {
+  return RZ * 32 * 16 + RZ * 32 * 8;
+}
 template <int RX, int RZ>
+__host__ __device__ constexpr int conv_tables_bytes() {
+  return fft_tables_bytes(RX, RZ) + ztabs_bytes<RZ>();
+}
+__host__ __device__ constexpr int conv_tables_bytes_rt(int RX, int RZ) {
+  return fft_tables_bytes(RX, RZ) + RZ * 32 * 16 + RZ * 32 * 8;
+}
+
+template <int RZ>
+__device__ __forceinline__ ZTabs build_ztabs(const ConvGeom& g, void* at) {
+  float4* zgc = reinterpret_cast<float4*>(at);
+  int2* zst = reinterpret_cast<int2*>(zgc + RZ * 32);
+  const int CZ = g.CZ, half = CZ >> 1;
+  for (int e = threadIdx.x; e < RZ * 32; e += blockDim.x) {
+    const int k1 = e >> 5, lz = (e & 31) & (CZ - 1);
+    int c;
+    float mx = 1.f, my = 0.f, sy = 1.f;
+    if (CZ == 1) {
+      c = 0;
+      sy = 0.f;
+    } else if ((lz & 1) == 0) {
+      c = k1 * half + (lz >> 1);
+      if (c == 0) sy = 0.f;
+    } else if (k1 == 0 && lz == 1) {
+      c = 0;
+      mx = 0.f;
+      my = 1.f;
+      sy = 0.f;
+    } else {
+      int lp, rp;
+      if (k1 > 0) {
+        lp = lz ^ (CZ - 1);
+        rp = RZ - k1;
+      } else {
+        lp = brev_rt((CZ - brev_rt(lz, g.logCZ)) & (CZ - 1), g.logCZ);
+        rp = 0;
+      }
+      c = rp * half + (lp >> 1);
+      sy = -1.f;
+    }
+    zgc[e] = make_float4(mx, my, sy, __int_as_float(c));
+    const int z = lz + CZ * k1 - g.padleft;
+    const int fl = ((z < 0 && z >= -g.hz) ? 1 : 0) | ((z >= g.nz && z < g.nz + g.hz) ? 2 : 0) | (z == 0 ? 4 : 0) |
+                   (z == g.nz - 1 ? 8 : 0);
+    zst[e] = make_int2((unsigned)z < (unsigned)g.nz ? z : -1, fl);
+  }
+  return ZTabs{zgc, zst};
+}
+
+// the z tables of a kernel with register counts RX, RZ (compile-time offset
+// from the dynamic shared memory base: no pointer registers)
+template <int RX, int RZ>
+__device__ __forceinline__ ZTabs ztabs_of() {
+  extern __shared__ float4 smem4[];
+  const float4* zgc = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(smem4) + fft_tables_bytes(RX, RZ));
+  return ZTabs{zgc, reinterpret_cast<const int2*>(zgc + RZ * 32)};
+}
+
+// shared memory: [FFT tables][z tables][B when bsmem]
+// ZT: build the z tables (kernels with a folding inverse z transform)
+template <int RX, int RZ, bool ZT = false>
 __device__ __forceinline__ float2* conv_setup(const Conv2Args& a, FftTables* T) {
   extern __shared__ float4 smem4[];
   float2* base = reinterpret_cast<float2*>(smem4);
   *T = build_fft_tables(base, a.tw, RX, a.g.logNpx, RZ, a.g.logNpz);
+  if (ZT) build_ztabs<RZ>(a.g, reinterpret_cast<char*>(smem4) + fft_tables_bytes(RX, RZ));
   __syncthreads();
-  if (a.bsmem) return base + fft_tables_bytes(RX, RZ) / 8;
+  if (a.bsmem) return base + conv_tables_bytes<RX, RZ>() / 8;
   return a.gB + (size_t)blockIdx.x * a.g.nx * a.g.QS;
 }
 
@@ -100,22 +178,39 @@ struct PlaneWalk {
   }
 };
 
+// visits the elements (k = z * nx + x) of an nz x nx plane that belong to
+// this thread; when nx divides blockDim.x each thread keeps one column x
+template <class F>
+__device__ __forceinline__ void plane_walk(const ConvGeom& g, const PlaneWalk& W, F f) {
+  const int nx = g.nx;
+  if (W.dx == 0) {
+    const int x = W.x0;
+#pragma unroll 2
+    for (int z = W.z0; z < g.nz; z += W.dz) f(z * nx + x, x, z);
+  } else {
+    const int n = g.nx * g.nz;
+    int x = W.x0, z = W.z0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      f(k, x, z);
+      x += W.dx;
+      z += W.dz;
+      if (x >= nx) {
+        x -= nx;
+        ++z;
+      }
+    }
+  }
+}
+
 // real nz x nx plane (x fastest) -> real rows of B, times the attenuation
 // plane `att` when given
 __device__ __forceinline__ void load_plane(const ConvGeom& g, const PlaneWalk& W, float2* B,
                                            const float* __restrict__ src, const float* __restrict__ att) {
   float* Bf = reinterpret_cast<float*>(B);
-  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
-  int x = W.x0, z = W.z0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+  const int rs = 2 * g.QS;
+  plane_walk(g, W, [&](int k, int x, int z) {
     Bf[x * rs + z] = att ? __fmul_rn(__ldg(src + k), __ldg(att + k)) : __ldg(src + k);
-    x += W.dx;
-    z += W.dz;
-    if (x >= nx) {
-      x -= nx;
-      ++z;
-    }
-  }
+  });
 }
 
 // real rows of B -> nz x nx plane (x fastest) in global memory, times the
@@ -123,17 +218,8 @@ __device__ __forceinline__ void load_plane(const ConvGeom& g, const PlaneWalk& W
 __device__ __forceinline__ void store_plane_satt(const ConvGeom& g, const PlaneWalk& W, const float2* B,
                                                  float* __restrict__ dst, const float* satt) {
   const float* Bf = reinterpret_cast<const float*>(B);
-  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
-  int x = W.x0, z = W.z0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    dst[k] = __fmul_rn(satt[k], Bf[x * rs + z]);
-    x += W.dx;
-    z += W.dz;
-    if (x >= nx) {
-      x -= nx;
-      ++z;
-    }
-  }
+  const int rs = 2 * g.QS;
+  plane_walk(g, W, [&](int k, int x, int z) { dst[k] = __fmul_rn(satt[k], Bf[x * rs + z]); });
 }
 
 // real rows of B -> nz x nx plane (x fastest) in global memory, times the
@@ -141,17 +227,10 @@ __device__ __forceinline__ void store_plane_satt(const ConvGeom& g, const PlaneW
 __device__ __forceinline__ void store_plane(const ConvGeom& g, const PlaneWalk& W, const float2* B,
                                             float* __restrict__ dst, const float* __restrict__ att) {
   const float* Bf = reinterpret_cast<const float*>(B);
-  const int nx = g.nx, n = g.nx * g.nz, rs = 2 * g.QS;
-  int x = W.x0, z = W.z0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+  const int rs = 2 * g.QS;
+  plane_walk(g, W, [&](int k, int x, int z) {
     dst[k] = att ? __fmul_rn(__ldg(att + k), Bf[x * rs + z]) : Bf[x * rs + z];
-    x += W.dx;
-    z += W.dz;
-    if (x >= nx) {
-      x -= nx;
-      ++z;
-    }
-  }
+  });
 }
 
 // Per-lane index tables, computed once per kernel.
@@ -280,9 +359,26 @@ __device__ __forceinline__ void zfft_rows_fwd(const ConvGeom& g, float2* B, cons
 }
 
 // Hermitian z-spectrum of the row pair from the stored columns, in the
-// scrambled input order of fft_inv: v = Z0 + i Z1 (gather codes: LaneTables::zg)
+// scrambled input order of fft_inv: v = Z0 + i Z1 (ZTabs::zgc + lane)
 template <int RZ>
-__device__ __forceinline__ void gather_zspec(const float2* b0, const float2* b1, const int (&zg)[RZ],
+__device__ __forceinline__ void gather_zspec(const float2* b0, const float2* b1, const float4* zgc,
+                                             float2 (&v)[RZ]) {
+#pragma unroll
+  for (int k1 = 0; k1 < RZ; ++k1) {
+    const float4 t = zgc[k1 * 32];
+    const int c = __float_as_int(t.w);
+    const float2 a = b0[c], b = b1[c];
+    const float ax = fmaf(t.x, a.x, t.y * a.y), ay = t.z * a.y;
+    const float bx = fmaf(t.x, b.x, t.y * b.y), by = t.z * b.y;
+    v[k1] = make_float2(ax - by, ay + bx);
+  }
+}
+
+// Hermitian z-spectrum of the row pair from the stored columns, in the
+// scrambled input order of fft_inv: v = Z0 + i Z1 (gather codes: LaneTables::zg;
+// the forward kernels' chunk-end inverse, where registers are scarcer)
+template <int RZ>
+__device__ __forceinline__ void gather_zspec_codes(const float2* b0, const float2* b1, const int (&zg)[RZ],
                                              float2 (&v)[RZ]) {
 #pragma unroll
   for (int k1 = 0; k1 < RZ; ++k1) {
@@ -314,8 +410,64 @@ __device__ __forceinline__ float2 group_sum(float2 s, int logC_rt) {
 // the edge samples.  Of the padded samples only the hz next to the image can
 // be non-zero (zero-padded input, PSF half width hz, no wrap-around since the
 // pads are >= hz), so only those are summed; the rest hold FFT round-off.
+// gather and store through the shared-memory z tables (ZTabs)
 template <int RZ, bool FOLD>
 __device__ __forceinline__ void zfft_rows_inv(const ConvGeom& g, float2* B, const FftTables& TT, int warp,
+                                              int lane, const ZTabs& Z) {
+  const Lanes L = lanes_of(lane, g.logCZ);
+  const int GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
+  const int npairs = g.nx >> 1, iters = (npairs + units - 1) / units;
+  float* Bf = reinterpret_cast<float*>(B);
+  const int rs = 2 * g.QS, QS = g.QS;
+  for (int it = 0; it < iters; ++it) {
+    const int rp = it * units + warp * GZ + L.g;
+    const bool active = rp < npairs;
+    const int x0 = 2 * min(rp, npairs - 1);
+    float2 v[RZ];
+    gather_zspec<RZ>(B + x0 * QS, B + (x0 + 1) * QS, Z.zgc + lane, v);
+    __syncwarp();
+    fft_inv<RZ>(v, L.l, g.logCZ, TT, TT.rz + L.l);
+    float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
+    if (FOLD) {
+#pragma unroll
+      for (int r = 0; r < RZ; ++r) {
+        const int fl = Z.zst[r * 32 + lane].y;
+        if (fl & 1) lo = cadd(lo, v[r]);
+        if (fl & 2) hi = cadd(hi, v[r]);
+      }
+      lo = group_sum<RZ>(lo, g.logCZ);
+      hi = group_sum<RZ>(hi, g.logCZ);
+    }
+    if (active) {
+      float* r0 = Bf + x0 * rs;
+      float* r1 = r0 + rs;
+#pragma unroll
+      for (int r = 0; r < RZ; ++r) {
+        const int2 e = Z.zst[r * 32 + lane];
+        const int z = e.x;
+        if (z >= 0) {
+          float2 w = v[r];
+          if (FOLD) {
+            if (e.y & 4) w = cadd(w, lo);
+            if (e.y & 8) w = cadd(w, hi);
+          }
+          r0[z] = w.x;
+          r1[z] = w.y;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// inverse z transform of row pairs: stored columns -> real rows (in place),
+// gathering with the register codes zg (the forward kernels' chunk end).
+// FOLD: adjoint of the replicate padding: the padded samples are summed into
+// the edge samples.  Of the padded samples only the hz next to the image can
+// be non-zero (zero-padded input, PSF half width hz, no wrap-around since the
+// pads are >= hz), so only those are summed; the rest hold FFT round-off.
+template <int RZ, bool FOLD>
+__device__ __forceinline__ void zfft_rows_inv_codes(const ConvGeom& g, float2* B, const FftTables& TT, int warp,
                                               int lane, const int (&zg)[RZ]) {
   const Lanes L = lanes_of(lane, g.logCZ);
   const int CZ = g.CZ, GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
@@ -327,7 +479,7 @@ __device__ __forceinline__ void zfft_rows_inv(const ConvGeom& g, float2* B, cons
     const bool active = rp < npairs;
     const int x0 = 2 * min(rp, npairs - 1);
     float2 v[RZ];
-    gather_zspec<RZ>(B + x0 * QS, B + (x0 + 1) * QS, zg, v);
+    gather_zspec_codes<RZ>(B + x0 * QS, B + (x0 + 1) * QS, zg, v);
     __syncwarp();
     fft_inv<RZ>(v, L.l, g.logCZ, TT, TT.rz + L.l);
     float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
@@ -478,16 +630,10 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
         phase ^= 1u;
         float* Bf = reinterpret_cast<float*>(B);
         const int rs = 2 * g.QS;
-        int x = W.x0, z = W.z0;
-        for (int k = threadIdx.x; k < nplane; k += blockDim.x) {
-          Bf[x * rs + z] = a.att_mul ? __fmul_rn(sP[k], sA[k]) : sP[k];
-          x += W.dx;
-          z += W.dz;
-          if (x >= g.nx) {
-            x -= g.nx;
-            ++z;
-          }
-        }
+        if (a.att_mul)
+          plane_walk(g, W, [&](int k, int x, int z) { Bf[x * rs + z] = __fmul_rn(sP[k], sA[k]); });
+        else
+          plane_walk(g, W, [&](int k, int x, int z) { Bf[x * rs + z] = sP[k]; });
         __syncthreads();
         if (threadIdx.x == 0) {  // prefetch the next plane of this CTA
           if (y + 1 < y1) issue(item, y + 1);
@@ -562,7 +708,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
       }
     }
     __syncthreads();
-    zfft_rows_inv<RZ, false>(g, B, TT, warp, lane, TW.zg);
+    zfft_rows_inv_codes<RZ, false>(g, B, TT, warp, lane, TW.zg);
     __syncthreads();
     store_plane(g, W, B, a.part + ((size_t)slot * a.nchunks + ch) * g.nz * g.nx, nullptr);
   }
@@ -611,13 +757,13 @@ template <int RX, int RZ, bool REGACC, bool STAGE>
 __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
   const ConvGeom& g = a.g;
   FftTables TT;
-  float2* B = conv_setup<RX, RZ>(a, &TT);
+  float2* B = conv_setup<RX, RZ, true>(a, &TT);
   // STAGE: the attenuation plane of each output plane is bulk-copied into
   // shared memory while the plane is transformed, and multiplied in on store.
   // Shared memory: [FFT tables][B when bsmem][attenuation plane][mbarrier]
   const int nplane = g.nz * g.nx;
   extern __shared__ float4 smem4[];
-  float* sA = reinterpret_cast<float*>(reinterpret_cast<char*>(smem4) + fft_tables_bytes(RX, RZ) +
+  float* sA = reinterpret_cast<float*>(reinterpret_cast<char*>(smem4) + conv_tables_bytes<RX, RZ>() +
                                        (a.bsmem ? sizeof(float2) * (size_t)g.nx * g.QS : 0));
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(sA + nplane);
   unsigned phase = 0;
@@ -697,7 +843,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
         }
       }
       __syncthreads();
-      zfft_rows_inv<RZ, true>(g, B, TT, warp, lane, T.zg);
+      zfft_rows_inv<RZ, true>(g, B, TT, warp, lane, ztabs_of<RX, RZ>());
       if (STAGE) {
         if (__syncthreads_or(!mbar_wait(bar, phase))) {
           if (threadIdx.x == 0) {

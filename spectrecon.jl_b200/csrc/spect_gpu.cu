@@ -321,7 +321,7 @@ int configure(spect_plan_s* p) {
   cg.logCZ = ilog2(cg.CZ);
   p->RX = g.Npx / cg.CX;
   p->RZ = g.Npz / cg.CZ;
-  size_t base = (size_t)fft_tables_bytes(p->RX, p->RZ);
+  size_t base = (size_t)conv_tables_bytes_rt(p->RX, p->RZ);
   size_t Bb = sizeof(float2) * (size_t)g.nx * cg.QS;
   p->conv_bsmem = (base + Bb <= p->max_smem) ? 1 : 0;
   p->conv_smem = base + (p->conv_bsmem ? Bb : 0);
