@@ -298,14 +298,25 @@ struct LaneTables {
 
 // z transform of row pairs (x0, x0+1), in place in B: real rows -> stored
 // columns.  ZEROPAD: zero padding (adjoint) instead of replication.
+// psrc0: source lane of register 0's spectrum partner (z_partner_lane).
+// Every lane stores its two unpacked values to a column: even lanes to
+// k1 * half + lane/2, odd lanes (whose values duplicate an even lane's
+// conjugates) to the unused column Q; lane 0 packs the Nyquist value of lane 1
+// beside the DC value in column 0.
+__device__ __forceinline__ int z_partner_lane(const ConvGeom& g, const Lanes& L) {
+  return L.gbase + brev_rt((g.CZ - brev_rt(L.l, g.logCZ)) & (g.CZ - 1), g.logCZ);
+}
+
 template <int RZ, bool ZEROPAD>
 __device__ __forceinline__ void zfft_rows_fwd(const ConvGeom& g, float2* B, const FftTables& TT, int warp,
-                                              int lane, const int (&zrd)[RZ]) {
+                                              int lane, const int (&zrd)[RZ], int psrc0) {
   const Lanes L = lanes_of(lane, g.logCZ);
-  const int CZ = g.CZ, GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
+  const int CZ = RZ > 1 ? 32 : g.CZ, GZ = 32 >> g.logCZ, units = kConvWarps * GZ;
   const int npairs = g.nx >> 1, iters = (npairs + units - 1) / units;
   float* Bf = reinterpret_cast<float*>(B);
   const int rs = 2 * g.QS, QS = g.QS, half = CZ >> 1;
+  const bool odd = (L.l & 1) != 0;
+  const int cbase = odd ? g.Q : (L.l >> 1);
   for (int it = 0; it < iters; ++it) {
     const int rp = it * units + warp * GZ + L.g;
     const bool active = rp < npairs;
@@ -321,36 +332,38 @@ __device__ __forceinline__ void zfft_rows_fwd(const ConvGeom& g, float2* B, cons
     }
     __syncwarp();
     fft_fwd<RZ>(v, L.l, g.logCZ, TT, TT.rz + L.l);
-    // partners: register k1 <-> RZ-k1 in lane l ^ (CZ-1); register 0 via brev
+    // partners: register k1 <-> RZ-k1 in lane l ^ (CZ-1); register 0 via psrc0
     float2 p[RZ];
-    p[0] = shfl2(v[0], L.gbase + brev_rt((CZ - brev_rt(L.l, g.logCZ)) & (CZ - 1), g.logCZ));
+    p[0] = shfl2(v[0], psrc0);
 #pragma unroll
     for (int k1 = 1; k1 < RZ; ++k1) p[k1] = shfl_xor2(v[RZ - k1], CZ - 1);
-    if (active) {
-      float2* b0 = B + x0 * QS;
-      float2* b1 = b0 + QS;
-      float* f0 = reinterpret_cast<float*>(b0);
-      float* f1 = reinterpret_cast<float*>(b1);
+    float2 A[RZ], Bb[RZ];
 #pragma unroll
-      for (int k1 = 0; k1 < RZ; ++k1) {
-        // two real rows from one complex transform
-        float2 A = make_float2(0.5f * (v[k1].x + p[k1].x), 0.5f * (v[k1].y - p[k1].y));
-        float2 Bb = make_float2(0.5f * (v[k1].y + p[k1].y), 0.5f * (p[k1].x - v[k1].x));
-        if (CZ == 1) {
-          b0[0] = make_float2(A.x, 0.f);
-          b1[0] = make_float2(Bb.x, 0.f);
-        } else if ((L.l & 1) == 0) {
-          const int c = k1 * half + (L.l >> 1);
-          if (c == 0) {
-            f0[0] = A.x;
-            f1[0] = Bb.x;
-          } else {
-            b0[c] = A;
-            b1[c] = Bb;
-          }
-        } else if (k1 == 0 && L.l == 1) {  // Nyquist, packed in column 0
-          f0[1] = A.x;
-          f1[1] = Bb.x;
+    for (int k1 = 0; k1 < RZ; ++k1) {
+      // two real rows from one complex transform
+      A[k1] = make_float2(0.5f * (v[k1].x + p[k1].x), 0.5f * (v[k1].y - p[k1].y));
+      Bb[k1] = make_float2(0.5f * (v[k1].y + p[k1].y), 0.5f * (p[k1].x - v[k1].x));
+    }
+    float2* b0 = B + x0 * QS;
+    float2* b1 = b0 + QS;
+    if (CZ == 1) {
+      if (active) {
+        b0[0] = make_float2(A[0].x, 0.f);
+        b1[0] = make_float2(Bb[0].x, 0.f);
+      }
+    } else {
+      const float nyA = __shfl_sync(0xffffffffu, A[0].x, L.gbase + 1);
+      const float nyB = __shfl_sync(0xffffffffu, Bb[0].x, L.gbase + 1);
+      if (L.l == 0) {
+        A[0].y = nyA;
+        Bb[0].y = nyB;
+      }
+      if (active) {
+#pragma unroll
+        for (int k1 = 0; k1 < RZ; ++k1) {
+          const int c = odd ? cbase : cbase + k1 * half;
+          b0[c] = A[k1];
+          b1[c] = Bb[k1];
         }
       }
     }
@@ -610,6 +623,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
   const PlaneWalk W(g.nx);
   LaneTables<RX, RZ> T;
   T.init(g, lane, false, true, false);
+  const int zp0 = z_partner_lane(g, lanes_of(lane, g.logCZ));
   for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
     const int slot = item / a.nchunks, ch = item - slot * a.nchunks;
     const int y0 = ch * a.chunkY, y1 = min(g.ny, y0 + a.chunkY);
@@ -646,7 +660,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_fwd2(Conv2Args a) {
                    a.att_mul ? a.att + ((size_t)a.vidx[slot] * g.ny + y) * g.nz * g.nx : nullptr);
         __syncthreads();
       }
-      zfft_rows_fwd<RZ, false>(g, B, TT, warp, lane, T.zrd);
+      zfft_rows_fwd<RZ, false>(g, B, TT, warp, lane, T.zrd, zp0);
       __syncthreads();
       const float* Hy = Hv + (size_t)y * (Q + 1) * Npx;
 #pragma unroll
@@ -729,11 +743,12 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
   const PlaneWalk W(g.nx);
   LaneTables<RX, RZ> T;
   T.init(g, lane, true);
+  const int zp0 = z_partner_lane(g, lanes_of(lane, g.logCZ));
   for (int slot = blockIdx.x; slot < a.nv; slot += gridDim.x) {
     __syncthreads();
     load_plane(g, W, B, a.views + (size_t)slot * g.nz * g.nx, nullptr);
     __syncthreads();
-    zfft_rows_fwd<RZ, true>(g, B, TT, warp, lane, T.zrd);
+    zfft_rows_fwd<RZ, true>(g, B, TT, warp, lane, T.zrd, zp0);
     __syncthreads();
     for (int it = 0; it < iters; ++it) {
       const int c = it * units + warp * GX + L.g;

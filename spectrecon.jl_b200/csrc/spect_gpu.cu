@@ -393,11 +393,12 @@ int configure(spect_plan_s* p) {
     // 1: whole slices (accumulator + two slices); 2: bands of output rows
     // (accumulator band + two chunks of kRotBandRows rows)
     const int as = acc_stride(g.nx);
-    const size_t rsm = ((size_t)acc_floats(g.ny, as) + 2 * slice) * sizeof(float) + 16;
+    const size_t ptab = sizeof(float2) * (size_t)(g.nx + g.ny);  // position tables
+    const size_t rsm = ((size_t)acc_floats(g.ny, as) + 2 * slice) * sizeof(float) + 16 + ptab;
     int nband = 0;
     size_t bsm = 0;
     for (int nb = 2; nb <= g.ny && ok && rsm > p->max_smem; ++nb) {
-      bsm = sizeof(float) * ((size_t)acc_floats(cdiv(g.ny, nb), as) + 2 * (size_t)kRotBandRows * g.nx) + 16;
+      bsm = sizeof(float) * ((size_t)acc_floats(cdiv(g.ny, nb), as) + 2 * (size_t)kRotBandRows * g.nx) + 16 + ptab;
       if (bsm <= p->max_smem) {
         nband = nb;
         break;

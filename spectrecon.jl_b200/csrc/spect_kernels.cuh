@@ -214,9 +214,27 @@ __device__ __forceinline__ ClassCols class_cols(int nx, int c1) {
   return w;
 }
 
-template <bool GUARD>
-__device__ __forceinline__ void scatter_class(const RotPos& R, const float* S, int nx, int r0, int nr, int c1,
-                                              int c2, const ClassCols& cw, float* acc, int as, int ya, int yb) {
+// rotated positions from per-view tables: PA[o1] = (cs (o1 - c0), sn (o1 - c0)),
+// PB[o2] = (sn (o2 - c0), cs (o2 - c0)), the products of RotPos::pos rounded
+// the same way, so s = c0 + (PA.x - PB.x, PA.y + PB.y) is bit-identical
+struct PosTab {
+  const float2* PA;
+  const float2* PB;
+};
+__device__ __forceinline__ void build_postab(const RotPos& R, int nx, int ny, float2* PA, float2* PB) {
+  for (int e = threadIdx.x; e < nx + ny; e += blockDim.x) {
+    const int o = e < nx ? e : e - nx;
+    const float d = __fsub_rn((float)o, R.c0);
+    if (e < nx) PA[o] = make_float2(__fmul_rn(R.cs, d), __fmul_rn(R.sn, d));
+    else PB[o] = make_float2(__fmul_rn(R.sn, d), __fmul_rn(R.cs, d));
+  }
+}
+
+// PTAB: positions from a PosTab (else RotPos::pos)
+template <bool GUARD, bool PTAB>
+__device__ __forceinline__ void scatter_class(const RotPos R, const PosTab PT, const float* S, int nx, int r0,
+                                              int nr, int c1, int c2, const ClassCols cw, float* acc, int as,
+                                              int ya, int yb) {
   const int o2f = r0 + (c2 - r0 % 3 + 3) % 3;
   const int nrow = o2f < r0 + nr ? (r0 + nr - 1 - o2f) / 3 + 1 : 0;
   const int npt = cw.npt, dq = cw.dq, dm = cw.dm;
@@ -243,7 +261,14 @@ __device__ __forceinline__ void scatter_class(const RotPos& R, const float* S, i
       const bool act = k ? hasb : true;
       val[k] = act ? S[(o2 - r0) * nx + o1] : 0.f;
       float s1, s2;
-      R.pos(o1, o2, s1, s2);
+      if (PTAB) {
+        // an inactive second point may lie past the last row: read row r0
+        const float2 pa = PT.PA[o1], pb = PT.PB[act ? o2 : r0];
+        s1 = __fadd_rn(R.c0, __fsub_rn(pa.x, pb.x));
+        s2 = __fadd_rn(R.c0, __fadd_rn(pa.y, pb.y));
+      } else {
+        R.pos(o1, o2, s1, s2);
+      }
       const float f1 = floorf(s1), f2 = floorf(s2);
       const int j1 = (int)f1, j2 = (int)f2;
       const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
@@ -388,7 +413,8 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj(Geom g, const flo
     //    pixels apart (|Rot (3a,3b)|_inf >= 3/sqrt 2), so they never overlap
     for (int cls = 0; cls < 9; ++cls) {
       const int c1 = cls % 3;
-      scatter_class<false>(R, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, nx, 0, ny);
+      scatter_class<false, false>(R, PosTab{}, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc,
+                                  nx, 0, ny);
       __syncthreads();
     }
   }
@@ -421,6 +447,8 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_stream(Geom g, co
   float* const Sb0 = reinterpret_cast<float*>(smem4) + acc_floats(ny, as);
   float* const Sb1 = Sb0 + slice;
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(Sb1 + slice);
+  float2* const PA = reinterpret_cast<float2*>(bar + 2);  // position tables (nx + ny)
+  float2* const PB = PA + nx;
   const int nitems = nz * nsplit;
   const int per = (nv + nsplit - 1) / nsplit;
   // next (item, slot) of this block after (it, s); it >= nitems when done
@@ -488,9 +516,12 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_stream(Geom g, co
     const float4 r = rot[vidx[s]];
     const RotPos R{r.x, r.y, g.c0};
     const float* S = b ? Sb1 : Sb0;
+    build_postab(R, nx, ny, PA, PB);
+    __syncthreads();
     for (int cls = 0; cls < 9; ++cls) {
       const int c1 = cls % 3;
-      scatter_class<true>(R, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, 0, ny);
+      scatter_class<true, true>(R, PosTab{PA, PB}, S, nx, 0, ny, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2,
+                                acc, as, 0, ny);
       __syncthreads();
     }
     if (it2 != it) {
@@ -531,6 +562,9 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
   float* const Sb0 = reinterpret_cast<float*>(smem4) + acc_floats(rows, as);
   float* const Sb1 = Sb0 + (size_t)CH * nx;
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(Sb1 + (size_t)CH * nx);
+  float2* const PA = reinterpret_cast<float2*>(bar + 2);  // position tables (nx + ny)
+  float2* const PB = PA + nx;
+  int s_tab = -1;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* outp = imgpart + (((size_t)split * nz + z) * ny + ya) * nx;
   const int nwarps = blockDim.x >> 5;
@@ -598,9 +632,15 @@ __global__ void __launch_bounds__(kRotAdjThreads, 1) k_rot_adj_band(Geom g, cons
     const RotPos R{r.x, r.y, c0};
     const int r0 = c * CH, nr = min(ny - r0, CH);
     const float* S = b ? Sb1 : Sb0;
+    if (s != s_tab) {  // new slot: its position tables
+      build_postab(R, nx, ny, PA, PB);
+      s_tab = s;
+      __syncthreads();
+    }
     for (int cls = 0; cls < 9; ++cls) {
       const int c1 = cls % 3;
-      scatter_class<true>(R, S, nx, r0, nr, c1, cls / 3, c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, ya, yb);
+      scatter_class<true, true>(R, PosTab{PA, PB}, S, nx, r0, nr, c1, cls / 3,
+                                c1 == 0 ? cw0 : c1 == 1 ? cw1 : cw2, acc, as, ya, yb);
       __syncthreads();
     }
     b ^= 1;
