@@ -225,6 +225,21 @@ int spect_plan_kernel_times(spect_plan_t plan, double ms[8], long long counts[8]
  * psf[px,pz,ny]).  fwhm_x/fwhm_z hold ny values (fwhm_z NULL = fwhm_x). */
 int spect_psf_gauss(float* psf, int ny, int px, int pz, const double* fwhm_x, const double* fwhm_z);
 
+/* psf_gauss on the device (src/psf-gauss.jl:24-55, with fwhm = range(start,
+ * end, ny) per axis): writes psf[ny][pz][px] (device memory of the caller)
+ * on `stream`, in double precision rounded to float like spect_psf_gauss. */
+int spect_psf_gauss_device(float* psf, int ny, int px, int pz, double fwhm_x_start, double fwhm_x_end,
+                           double fwhm_z_start, double fwhm_z_end, void* stream);
+
+/* SPECTplan with the Gaussian PSF stack psf_gauss(; ny, px, pz, fwhm ranges)
+ * for every view (the repeated-PSF use of docs/lit/examples/1-overview.jl:
+ * 91-104), generated on the device: no host PSF array, one stack of PSF
+ * spectra.  Otherwise as spect_plan_create. */
+int spect_plan_create_gauss(spect_plan_t* plan, int nx, int ny, int nz, int px, int pz, int nview,
+                            const float* mumap, double fwhm_x_start, double fwhm_x_end, double fwhm_z_start,
+                            double fwhm_z_end, float dy, const float* viewangle, int interpmeth, int mode,
+                            int nthread, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -37,7 +37,7 @@ from ._native import SpectError, check
 
 __all__ = [
     "Batch", "Server", "SPECTplan", "project", "project_", "backproject", "backproject_", "mlem", "mlem_", "osem", "osem_",
-    "Ablock", "psf_gauss", "nthreads", "SpectError",
+    "Ablock", "psf_gauss", "psf_gauss_device", "nthreads", "SpectError",
 ]
 
 
@@ -134,6 +134,43 @@ class SPECTplan:
             ctypes.byref(h), nx, ny, nz, px, pz, nview, _ptr(mu), _ptr(ps), float(self.dy),
             None if ang is None else _ptr(ang), self.interpmeth, self.mode, self.nthread, nthreads()))
         self._h = h
+
+    @classmethod
+    def gauss(cls, mumap, dy, nview, px=11, pz=None, fwhm_start=1.0, fwhm_end=4.0, fwhm_z_start=None,
+              fwhm_z_end=None, viewangle=None, interpmeth="two", nthread=None, mode="fast"):
+        """SPECTplan(mumap, repeat(psf_gauss(; ny, px, pz, fwhm_start, fwhm_end),
+        nview), dy) without building the PSF array: the Gaussian stack is
+        generated on the GPU (spect_plan_create_gauss) and shared by all views."""
+        pz = px if pz is None else pz
+        fz0 = fwhm_start if fwhm_z_start is None else fwhm_z_start
+        fz1 = fwhm_end if fwhm_z_end is None else fwhm_z_end
+        mumap = np.asarray(mumap)
+        if mumap.ndim != 3:
+            raise SpectError(8, "DimensionMismatch: mumap must be 3-D")
+        nx, ny, nz = mumap.shape
+        self = cls.__new__(cls)
+        self.T = np.float32
+        self.imgsize = (nx, ny, nz)
+        self.px, self.pz, self.nview = int(px), int(pz), int(nview)
+        self.dy = np.float32(dy)
+        self.interpmeth = {"one": 1, ":one": 1, 1: 1, "two": 2, ":two": 2, 2: 2}.get(interpmeth, -1)
+        self.mode = {"fast": 0, ":fast": 0, "mem": 1, ":mem": 1}.get(mode, -1)
+        self.nthread = nthreads() if nthread is None else int(nthread)
+        mu = np.asfortranarray(mumap, dtype=np.float32)
+        ang = None
+        if viewangle is not None:
+            ang = np.ascontiguousarray(np.asarray(viewangle, dtype=np.float32).ravel())
+            if ang.size != nview:
+                raise SpectError(8, "DimensionMismatch: viewangle must have nview entries")
+        self.viewangle = ang
+        h = ctypes.c_void_p()
+        self._h = None
+        check(_native.lib().spect_plan_create_gauss(
+            ctypes.byref(h), nx, ny, nz, int(px), int(pz), int(nview), _ptr(mu), float(fwhm_start),
+            float(fwhm_end), float(fz0), float(fz1), float(self.dy), None if ang is None else _ptr(ang),
+            self.interpmeth, self.mode, self.nthread, nthreads()))
+        self._h = h
+        return self
 
     @property
     def handle(self):
@@ -439,3 +476,17 @@ def psf_gauss(ny=128, px=11, pz=None, fwhm_start=1, fwhm_end=4, fwhm=None, fwhm_
     out = np.empty((px, pz, ny), dtype=np.float32, order="F")
     check(_native.lib().spect_psf_gauss(_ptr(out), int(ny), int(px), int(pz), _ptr(fx), _ptr(fz)))
     return out.astype(T, order="F")
+
+
+def psf_gauss_device(out, ny=128, px=11, pz=None, fwhm_start=1.0, fwhm_end=4.0, fwhm_z_start=None,
+                     fwhm_z_end=None, stream=None):
+    """psf_gauss(; ny, px, pz, fwhm_start, fwhm_end) written on the GPU into
+    ``out``, a float32 device array of shape (px, pz, ny) in column-major
+    order (no host array, no allocation); returns ``out``."""
+    pz = px if pz is None else pz
+    fz0 = fwhm_start if fwhm_z_start is None else fwhm_z_start
+    fz1 = fwhm_end if fwhm_z_end is None else fwhm_z_end
+    p = _dev_ptr(out, (px, pz, ny), "psf")
+    check(_native.lib().spect_psf_gauss_device(p, int(ny), int(px), int(pz), float(fwhm_start), float(fwhm_end),
+                                               float(fz0), float(fz1), _stream_ptr(stream)))
+    return out

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libspectgpu.so")
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _F = ctypes.c_float
+_D = ctypes.c_double
 _Z = ctypes.c_size_t
 
 class JobDesc(ctypes.Structure):
@@ -57,6 +58,8 @@ _SIGS = {
     "spect_plan_profile": ([_P, _I], _I),
     "spect_plan_kernel_times": ([_P, _P, _P], _I),
     "spect_psf_gauss": ([_P, _I, _I, _I, _P, _P], _I),
+    "spect_psf_gauss_device": ([_P, _I, _I, _I, _D, _D, _D, _D, _P], _I),
+    "spect_plan_create_gauss": ([_P, _I, _I, _I, _I, _I, _I, _P, _D, _D, _D, _D, _F, _P, _I, _I, _I, _I], _I),
 }
 
 _lib = None

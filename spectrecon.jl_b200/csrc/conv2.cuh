@@ -65,6 +65,7 @@ struct Conv2Args {
   const float* att;     // attenuation cache [view][y][z][x]; att_mul: applied on plane load (forward)
   int att_mul;
   int* err;             // set to 1 when a bounded wait gives up
+  int vsplit;           // k_vspec2: column blocks per view (work items nv * vsplit)
 };
 
 struct Lanes {
@@ -87,27 +88,43 @@ __device__ __forceinline__ Lanes lanes_of(int lane, int logC) {
 //   zst  output sample z of register r: (z, or -1 outside the image; flags
 //        1: z in the low fold range, 2: high fold range, 4: z == 0,
 //        8: z == nz - 1)
+//   xfl  per lane, bit r of: x of register r of the inverse x transform in
+//        the low fold range, the high fold range, x == 0, x == nx - 1
 struct ZTabs {
   const float4* zgc;
   const int2* zst;
+  const int4* xfl;
 };
 
 template <int RZ>
 __host__ __device__ constexpr int ztabs_bytes() {
-  return RZ * 32 * 16 + RZ * 32 * 8;
+  return RZ * 32 * 16 + RZ * 32 * 8 + 32 * 16;
 }
 template <int RX, int RZ>
 __host__ __device__ constexpr int conv_tables_bytes() {
   return fft_tables_bytes(RX, RZ) + ztabs_bytes<RZ>();
 }
 __host__ __device__ constexpr int conv_tables_bytes_rt(int RX, int RZ) {
-  return fft_tables_bytes(RX, RZ) + RZ * 32 * 16 + RZ * 32 * 8;
+  return fft_tables_bytes(RX, RZ) + RZ * 32 * 16 + RZ * 32 * 8 + 32 * 16;
 }
 
-template <int RZ>
+template <int RX, int RZ>
 __device__ __forceinline__ ZTabs build_ztabs(const ConvGeom& g, void* at) {
   float4* zgc = reinterpret_cast<float4*>(at);
   int2* zst = reinterpret_cast<int2*>(zgc + RZ * 32);
+  int4* xfl = reinterpret_cast<int4*>(zst + RZ * 32);
+  for (int l = threadIdx.x; l < 32; l += blockDim.x) {
+    const int CX = (RX > 1) ? 32 : g.CX, lx = l & (CX - 1);
+    int lo = 0, hi = 0, first = 0, last = 0;
+    for (int r = 0; r < RX; ++r) {
+      const int x = lx + CX * r - g.padup;
+      lo |= (x < 0 && x >= -g.hx) << r;
+      hi |= (x >= g.nx && x < g.nx + g.hx) << r;
+      first |= (x == 0) << r;
+      last |= (x == g.nx - 1) << r;
+    }
+    xfl[l] = make_int4(lo, hi, first, last);
+  }
   const int CZ = g.CZ, half = CZ >> 1;
   for (int e = threadIdx.x; e < RZ * 32; e += blockDim.x) {
     const int k1 = e >> 5, lz = (e & 31) & (CZ - 1);
@@ -142,7 +159,7 @@ __device__ __forceinline__ ZTabs build_ztabs(const ConvGeom& g, void* at) {
                    (z == g.nz - 1 ? 8 : 0);
     zst[e] = make_int2((unsigned)z < (unsigned)g.nz ? z : -1, fl);
   }
-  return ZTabs{zgc, zst};
+  return ZTabs{zgc, zst, xfl};
 }
 
 // the z tables of a kernel with register counts RX, RZ (compile-time offset
@@ -151,7 +168,8 @@ template <int RX, int RZ>
 __device__ __forceinline__ ZTabs ztabs_of() {
   extern __shared__ float4 smem4[];
   const float4* zgc = reinterpret_cast<const float4*>(reinterpret_cast<const char*>(smem4) + fft_tables_bytes(RX, RZ));
-  return ZTabs{zgc, reinterpret_cast<const int2*>(zgc + RZ * 32)};
+  const int2* zst = reinterpret_cast<const int2*>(zgc + RZ * 32);
+  return ZTabs{zgc, zst, reinterpret_cast<const int4*>(zst + RZ * 32)};
 }
 
 // shared memory: [FFT tables][z tables][B when bsmem]
@@ -161,7 +179,7 @@ __device__ __forceinline__ float2* conv_setup(const Conv2Args& a, FftTables* T) 
   extern __shared__ float4 smem4[];
   float2* base = reinterpret_cast<float2*>(smem4);
   *T = build_fft_tables(base, a.tw, RX, a.g.logNpx, RZ, a.g.logNpz);
-  if (ZT) build_ztabs<RZ>(a.g, reinterpret_cast<char*>(smem4) + fft_tables_bytes(RX, RZ));
+  if (ZT) build_ztabs<RX, RZ>(a.g, reinterpret_cast<char*>(smem4) + fft_tables_bytes(RX, RZ));
   __syncthreads();
   if (a.bsmem) return base + conv_tables_bytes<RX, RZ>() / 8;
   return a.gB + (size_t)blockIdx.x * a.g.nx * a.g.QS;
@@ -739,25 +757,28 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_vspec2(Conv2Args a) {
   float2* const xw = TT.xscr ? TT.xscr + warp * kXScr : nullptr;  // x-transform scratch
   const Lanes L = lanes_of(lane, g.logCX);
   const int CX = (RX > 1) ? 32 : g.CX, GX = 32 / CX, units = kConvWarps * GX, Q = g.Q, Npx = g.Npx;
-  const int iters = (Q + units - 1) / units;
   const PlaneWalk W(g.nx);
   LaneTables<RX, RZ> T;
   T.init(g, lane, true);
   const int zp0 = z_partner_lane(g, lanes_of(lane, g.logCZ));
-  for (int slot = blockIdx.x; slot < a.nv; slot += gridDim.x) {
+  // work item = (slot, block of columns): the z transforms are repeated per
+  // block so that a few views still spread over the whole GPU
+  const int vs = max(1, a.vsplit), cpb = (Q + vs - 1) / vs;
+  for (int item = blockIdx.x; item < a.nv * vs; item += gridDim.x) {
+    const int slot = item / vs, cb0 = (item - slot * vs) * cpb, cb1 = min(Q, cb0 + cpb);
     __syncthreads();
     load_plane(g, W, B, a.views + (size_t)slot * g.nz * g.nx, nullptr);
     __syncthreads();
     zfft_rows_fwd<RZ, true>(g, B, TT, warp, lane, T.zrd, zp0);
     __syncthreads();
-    for (int it = 0; it < iters; ++it) {
-      const int c = it * units + warp * GX + L.g;
-      const int cc = min(c, Q - 1);
+    for (int it = 0; it * units < cb1 - cb0; ++it) {
+      const int c = cb0 + it * units + warp * GX + L.g;
+      const int cc = min(c, cb1 - 1);
       float2 v[RX];
 #pragma unroll
       for (int r = 0; r < RX; ++r) v[r] = (T.xrd[r] >= 0) ? B[T.xrd[r] + cc] : make_float2(0.f, 0.f);
       fftx_fwd<RX>(v, L.l, g.logCX, TT, TT.rx + L.l, xw);
-      if (c < Q) {
+      if (c < cb1) {
         float2* o = a.VsOut + ((size_t)slot * Q + c) * Npx + L.l;
 #pragma unroll
         for (int k1 = 0; k1 < RX; ++k1) o[k1 * CX] = v[k1];
@@ -833,13 +854,13 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
           apply_psf<RX>(v, Hy + (size_t)cc * Npx + L.l, Hy + (size_t)Q * Npx + L.l, L, g.logCX,
                         j == 0 && warp == 0, cc == 0);
           fftx_inv<RX>(v, L.l, g.logCX, TT, TT.rx + L.l, xw);
-          // adjoint of the replicate padding along x
+          // adjoint of the replicate padding along x (fold masks: ZTabs::xfl)
+          const int4 xm = ztabs_of<RX, RZ>().xfl[lane];
           float2 lo = make_float2(0.f, 0.f), hi = make_float2(0.f, 0.f);
 #pragma unroll
           for (int r = 0; r < RX; ++r) {
-            int x = L.l + CX * r - g.padup;
-            if (x < 0 && x >= -g.hx) lo = cadd(lo, v[r]);
-            else if (x >= g.nx && x < g.nx + g.hx) hi = cadd(hi, v[r]);
+            if ((xm.x >> r) & 1) lo = cadd(lo, v[r]);
+            if ((xm.y >> r) & 1) hi = cadd(hi, v[r]);
           }
           lo = group_sum<RX>(lo, g.logCX);
           hi = group_sum<RX>(hi, g.logCX);
@@ -849,8 +870,8 @@ __global__ void __launch_bounds__(kConvThreads, 1) k_conv_adj2(Conv2Args a) {
               const int off = T.xwr[r];
               if (off >= 0) {
                 float2 w = v[r];
-                if (off == 0) w = cadd(w, lo);
-                if (off == (g.nx - 1) * g.QS) w = cadd(w, hi);
+                if ((xm.z >> r) & 1) w = cadd(w, lo);
+                if ((xm.w >> r) & 1) w = cadd(w, hi);
                 B[off + c] = w;
               }
             }

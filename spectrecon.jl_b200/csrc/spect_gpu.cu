@@ -558,7 +558,8 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     a.VsOut = p->d_Vs;
     a.nv = nv;
     a.vidx = vi;
-    LAUNCH(p, K_VSPEC, st, "k_vspec", conv_launch(p, 2, std::min(p->conv_grid, nv), st, a));
+    a.vsplit = std::max(1, std::min(8, cdiv(p->conv_grid, nv)));
+    LAUNCH(p, K_VSPEC, st, "k_vspec", conv_launch(p, 2, std::min(p->conv_grid, nv * a.vsplit), st, a));
     int cy, nc;
     chunking(p, nv, true, &cy, &nc);
     a.Vs = p->d_Vs;
@@ -954,6 +955,9 @@ struct PlanOpts {
   // view_set[v] names the stack of view v (already checked for symmetry)
   const int* view_set = nullptr;
   int nset = 0;
+  // Gaussian PSFs generated on the device (psfs unused): FWHM ranges along y
+  bool gauss = false;
+  double gx0 = 0, gx1 = 0, gz0 = 0, gz1 = 0;
 };
 
 // distinct PSF stacks of nview views (stack = ny*pp floats each): view_set[v]
@@ -991,7 +995,7 @@ bool psf_symmetric(const float* psfs, const std::vector<int>& stacks, size_t ny,
 int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview, const float* mumap,
                      const float* psfs, float dy, const float* viewangle, int interpmeth, int mode, int nthread,
                      int nthreads, const PlanOpts& opts) {
-  if (!out || !mumap || !psfs) return fail(SPECT_ERR_ARG, "null pointer argument");
+  if (!out || !mumap || (!psfs && !opts.gauss)) return fail(SPECT_ERR_ARG, "null pointer argument");
   *out = nullptr;
   if (nx <= 0 || ny <= 0 || nz <= 0 || px <= 0 || pz <= 0 || nview <= 0)
     return fail(SPECT_ERR_ARG, "sizes must be positive");
@@ -1003,7 +1007,10 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
   // distinct PSF stacks first: identical stacks are symmetric together
   const size_t stack = (size_t)ny * pp;
   std::vector<int> view_set, uniq;
-  if (opts.view_set) {
+  if (opts.gauss) {  // one generated stack for every view (symmetric by construction)
+    view_set.assign(nview, 0);
+    uniq.push_back(0);
+  } else if (opts.view_set) {
     view_set.assign(opts.view_set, opts.view_set + nview);
     for (int u = 0; u < opts.nset; ++u) uniq.push_back(u);  // stack u of the compact array
   } else {
@@ -1233,12 +1240,17 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     std::vector<float> hp(pp * batch);
     for (size_t b0 = 0; e == cudaSuccess && b0 < nplanes; b0 += batch) {
       size_t nb = std::min(batch, nplanes - b0);
-      for (size_t q = 0; q < nb; ++q) {
-        size_t pl = b0 + q;
-        size_t set = pl / ny, y = pl % ny;
-        std::memcpy(hp.data() + q * pp, psfs + ((size_t)uniq[set] * ny + y) * pp, sizeof(float) * pp);
+      if (opts.gauss) {  // planes b0.. of the single generated stack
+        const int gb = std::min(cdiv((long long)nb * pp, 256), p->sm_count * 16);
+        k_psf_gauss<<<gb, 256, 0, hs>>>(d_psf, (int)b0, (int)nb, ny, px, pz, opts.gx0, opts.gx1, opts.gz0, opts.gz1);
+      } else {
+        for (size_t q = 0; q < nb; ++q) {
+          size_t pl = b0 + q;
+          size_t set = pl / ny, y = pl % ny;
+          std::memcpy(hp.data() + q * pp, psfs + ((size_t)uniq[set] * ny + y) * pp, sizeof(float) * pp);
+        }
+        e = cudaMemcpyAsync(d_psf, hp.data(), sizeof(float) * pp * nb, cudaMemcpyHostToDevice, hs);
       }
-      e = cudaMemcpyAsync(d_psf, hp.data(), sizeof(float) * pp * nb, cudaMemcpyHostToDevice, hs);
       if (e != cudaSuccess) break;
       int blocks = std::min(cdiv((long long)nb * pz * Npx, 256), p->sm_count * 32);
       k_psf_stage1<<<blocks, 256, 0, hs>>>(d_psf, (int)nb, px, pz, Npx, d_wx, d_G);
@@ -1588,6 +1600,32 @@ int spect_psf_gauss(float* psf, int ny, int px, int pz, const double* fwhm_x, co
       for (int i = 0; i < px; ++i) psf[((size_t)y * pz + j) * px + i] = (float)(wx[i] * wz[j]);
   }
   return SPECT_OK;
+}
+
+int spect_psf_gauss_device(float* psf, int ny, int px, int pz, double fwhm_x_start, double fwhm_x_end,
+                           double fwhm_z_start, double fwhm_z_end, void* stream) {
+  if (!psf || ny <= 0 || px <= 0 || pz <= 0) return fail(SPECT_ERR_ARG, "bad psf_gauss arguments");
+  if (!(px % 2) || !(pz % 2)) return fail(SPECT_ERR_PSF_NOT_ODD, "non-odd size psfs");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const long long n = (long long)ny * px * pz;
+  k_psf_gauss<<<(int)std::min<long long>(cdiv(n, 256), (long long)sms * 16), 256, 0, (cudaStream_t)stream>>>(
+      psf, 0, ny, ny, px, pz, fwhm_x_start, fwhm_x_end, fwhm_z_start, fwhm_z_end);
+  return check_launch("k_psf_gauss");
+}
+
+int spect_plan_create_gauss(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview,
+                            const float* mumap, double fwhm_x_start, double fwhm_x_end, double fwhm_z_start,
+                            double fwhm_z_end, float dy, const float* viewangle, int interpmeth, int mode,
+                            int nthread, int nthreads) {
+  PlanOpts o;
+  o.gauss = true;
+  o.gx0 = fwhm_x_start;
+  o.gx1 = fwhm_x_end;
+  o.gz0 = fwhm_z_start;
+  o.gz1 = fwhm_z_end;
+  return plan_create_impl(out, nx, ny, nz, px, pz, nview, mumap, nullptr, dy, viewangle, interpmeth, mode, nthread,
+                          nthreads, o);
 }
 
 }  // extern "C"

@@ -664,6 +664,40 @@ __global__ void k_reduce_image(const float* __restrict__ imgpart, int nsplit, si
   }
 }
 
+// psf_gauss on the device (src/psf-gauss.jl:24-55) for planes y in
+// [y0, y0 + n): psf[y - y0][j][i] = wx[i] * wz[j], each axis a normalised
+// Gaussian exp(-r^2 / (2 sigma^2)), sigma = fwhm / sqrt(log 256), r = -h..h;
+// fwhm = 0 gives the Kronecker impulse.  fwhm(y) = start + y * (end - start)
+// / (ny - 1) (end exactly at y = ny - 1), in double as the host generator
+// (numpy.linspace's rule).  One thread per tap.
+__device__ __forceinline__ double gauss_fwhm(int y, int ny, double a, double b) {
+  if (ny <= 1) return a;
+  return y == ny - 1 ? b : a + y * ((b - a) / (ny - 1));
+}
+__device__ double gauss_tap(int r, int p, double fwhm) {
+  const int h = (p - 1) / 2;
+  if (fwhm == 0.0) return r == 0 ? 1.0 : 0.0;
+  const double sigma = fwhm / sqrt(log(256.0));
+  double s = 0.0;
+  for (int i = 0; i < p; ++i) {
+    const double q = (double)(-h + i) / sigma;
+    s += exp(-0.5 * q * q);
+  }
+  const double q = (double)r / sigma;
+  return exp(-0.5 * q * q) / s;
+}
+__global__ void k_psf_gauss(float* __restrict__ psf, int y0, int n, int ny, int px, int pz, double x0, double x1,
+                            double z0, double z1) {
+  const size_t pp = (size_t)px * pz, total = (size_t)n * pp;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+    const int y = y0 + (int)(k / pp);
+    const int e = (int)(k % pp), j = e / px, i = e - j * px;
+    const double wx = gauss_tap(i - (px - 1) / 2, px, gauss_fwhm(y, ny, x0, x1));
+    const double wz = gauss_tap(j - (pz - 1) / 2, pz, gauss_fwhm(y, ny, z0, z1));
+    psf[k] = (float)(wx * wz);
+  }
+}
+
 // ------------------------------------------------------------------------
 // PSF spectra: H[set][y][kz][kx] = Re sum_{d,e} h[d,e] w_x^{kx d} w_z^{kz e} / (Npx Npz)
 // with h[d,e] = psf[(pz-1)/2+e][(px-1)/2+d], the circularly centred kernel
