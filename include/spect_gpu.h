@@ -88,6 +88,13 @@ int spect_plan_destroy(spect_plan_t plan);
  * bytes held by the plan. */
 int spect_plan_info(spect_plan_t plan, int out[8], size_t* bytes);
 
+/* Convolution kernels of the plan (no reference counterpart: the reference
+ * always convolves by FFT, src/fft_convolve.jl:33-130).  out[0], out[1]: the
+ * direct separable kernels can run for the forward / adjoint (every PSF plane
+ * is rank-1); out[2], out[3]: the forward / adjoint currently uses them
+ * (1) or the FFT kernels (0).  spect_plan_autotune keeps the faster. */
+int spect_plan_conv_kernels(spect_plan_t plan, int out[4]);
+
 /* project!(views, image, plan; index) (src/project.jl:143-163).
  * views[nindex][nz][nx] = P_{index[i]} image; index NULL = all views in order
  * (nindex must then be nview).  Device pointers, enqueued on stream. */

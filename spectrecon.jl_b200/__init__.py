@@ -185,6 +185,17 @@ class SPECTplan:
         d["device_bytes"] = b.value
         return d
 
+    def conv_kernels(self):
+        """Which convolution kernels the plan runs: {"forward": "direct" |
+        "fft", "adjoint": ..., "direct_forward_ok": bool, "direct_adjoint_ok":
+        bool}.  Direct kernels need rank-1 (separable) PSF planes; autotune()
+        keeps whichever is faster for each direction."""
+        out = (ctypes.c_int * 4)()
+        check(_native.lib().spect_plan_conv_kernels(self._h, out))
+        name = ("fft", "direct")
+        return {"forward": name[out[2]], "adjoint": name[out[3]],
+                "direct_forward_ok": bool(out[0]), "direct_adjoint_ok": bool(out[1])}
+
     def autotune(self, nindex=None):
         """Time candidate launch shapes for calls with nindex views (default
         nview) and keep the fastest; returns (forward_ms, adjoint_ms)."""

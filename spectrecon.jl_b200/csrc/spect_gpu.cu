@@ -38,6 +38,7 @@
 #include "../../include/spect_gpu.h"
 #include "conv2.cuh"
 #include "rot_one.cuh"
+#include "sconv.cuh"
 #include "spect_kernels.cuh"
 
 using namespace spect;
@@ -183,6 +184,15 @@ struct spect_plan_s {
   float* d_imgpart = nullptr;
   float2* d_gB = nullptr;
   float2* d_gacc = nullptr;
+  // separable PSF planes: direct-FMA convolution (sconv.cuh)
+  // sep_fwd_ok / sep_adj_ok: the direct kernels can run; sep / sep_adj: they
+  // are in use (default on; the autotuner keeps the faster of direct and FFT)
+  int sep_ok = 0, sep = 0, sep_adj = 0, sep_hs = 0, sep_ts = 0;
+  int sep_shape_fwd = -1, sep_shape_adj = -1;  // indices into kSepShapes
+  int sep_fwd_ok = 0, sep_adj_ok = 0, sep_forced = 0;  // forced: 1 FFT, 2 direct
+  float* d_Hsep = nullptr;      // [nset][ny][sep_hs] reversed z, x factors
+  float* d_Tsep = nullptr;      // [nset][ny][sep_ts] adjoint edge tails
+  size_t sep_fwd_smem = 0, sep_adj_smem = 0;
   float* d_gscr_adj = nullptr;
   // EM scratch (lazily allocated)
   float* d_views_tmp = nullptr;  // [nview][nz][nx]
@@ -243,7 +253,7 @@ void free_plan(spect_plan_s* p) {
   void* ptrs[] = {p->d_mumap, p->d_att, p->d_err, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
-                  p->d_io_img, p->d_io_views};
+                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep};
   for (void* q : ptrs)
     if (q) {
       if (p->async_alloc) cudaFreeAsync(q, p->home);
@@ -465,6 +475,37 @@ Conv2Args conv_args(const spect_plan_s* p) {
   return a;
 }
 
+// k_sconv_fwd / k_sconv_adj instantiations, in kSepShapes order
+#define SEP_SHAPES(K)                                                                                   \
+  {(const void*)K<1, 512>, (const void*)K<2, 512>, (const void*)K<3, 512>, (const void*)K<4, 512>,   \
+   (const void*)K<5, 512>, (const void*)K<6, 512>, (const void*)K<1, 640>, (const void*)K<2, 640>,   \
+   (const void*)K<3, 640>, (const void*)K<4, 640>}
+const void* const kSconvFwd[kSepNShapes] = SEP_SHAPES(k_sconv_fwd);
+const void* const kSconvAdj[kSepNShapes] = SEP_SHAPES(k_sconv_adj);
+#undef SEP_SHAPES
+
+cudaError_t sep_launch(const void* const* table, int shape, int grid, size_t smem, cudaStream_t st, SepArgs a) {
+  void* args[] = {&a};
+  return cudaLaunchKernel(table[shape], dim3(grid), dim3(kSepShapes[shape].nth), args, smem, st);
+}
+
+SepArgs sep_args(const spect_plan_s* p) {
+  SepArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.nx = p->g.nx;
+  a.ny = p->g.ny;
+  a.nz = p->g.nz;
+  a.px = p->px;
+  a.pz = p->pz;
+  a.att = p->d_att;
+  a.att_mul = (p->d_att && p->interp == SPECT_INTERP_TWO) ? 1 : 0;
+  a.H = p->d_Hsep;
+  a.hs = p->sep_hs;
+  a.viewset = p->d_viewset;
+  a.err = p->d_err;
+  return a;
+}
+
 cudaError_t conv_launch(const spect_plan_s* p, int kind, int grid, cudaStream_t st, const Conv2Args& a,
                         size_t smem = 0) {
   if (!smem) smem = p->conv_smem;
@@ -524,6 +565,18 @@ int forward_scratch(spect_plan_s* p, float* views, const float* image, const int
     a.nchunks = nc;
     a.part = partbuf;
     int gridc = std::min(p->conv_grid, nv * nc);
+    if (p->sep) {
+      SepArgs sa = sep_args(p);
+      sa.P = Pbuf;
+      sa.vidx = vi;
+      sa.nv = nv;
+      sa.chunkY = cy;
+      sa.nchunks = nc;
+      sa.part = partbuf;
+      const int gs = std::min(p->sm_count, nv * nc);
+      const size_t sm = p->sep_fwd_smem;
+      LAUNCH(p, K_CONV_FWD, st, "k_sconv_fwd", sep_launch(kSconvFwd, p->sep_shape_fwd, gs, sm, st, sa));
+    } else
     LAUNCH(p, K_CONV_FWD, st, "k_conv_fwd",
            conv_launch(p, p->conv_stage ? 3 : 0, gridc, st, a, p->conv_stage ? p->conv_smem_fwd : p->conv_smem));
     // chunk sum (+ EM ratio) -> views
@@ -558,16 +611,32 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     a.VsOut = p->d_Vs;
     a.nv = nv;
     a.vidx = vi;
-    a.vsplit = std::max(1, std::min(8, cdiv(p->conv_grid, nv)));
-    LAUNCH(p, K_VSPEC, st, "k_vspec", conv_launch(p, 2, std::min(p->conv_grid, nv * a.vsplit), st, a));
     int cy, nc;
     chunking(p, nv, true, &cy, &nc);
-    a.Vs = p->d_Vs;
-    a.T = p->d_P;
-    a.chunkY = cy;
-    a.nchunks = nc;
-    LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj",
-           conv_launch(p, p->adj_stage ? 4 : 1, std::min(p->conv_grid, nv * nc), st, a, p->conv_smem_adj));
+    if (p->sep_adj) {
+      SepArgs sa = sep_args(p);
+      sa.att_mul = p->adj_stage ? 1 : 0;
+      sa.tails = p->d_Tsep;
+      sa.ts = p->sep_ts;
+      sa.views = views + (size_t)g0 * p->nxz;
+      sa.T = p->d_P;
+      sa.vidx = vi;
+      sa.nv = nv;
+      sa.chunkY = cy;
+      sa.nchunks = nc;
+      const int gs = std::min(p->sm_count, nv * nc);
+      const size_t sm = p->sep_adj_smem;
+      LAUNCH(p, K_CONV_ADJ, st, "k_sconv_adj", sep_launch(kSconvAdj, p->sep_shape_adj, gs, sm, st, sa));
+    } else {
+      a.vsplit = std::max(1, std::min(8, cdiv(p->conv_grid, nv)));
+      LAUNCH(p, K_VSPEC, st, "k_vspec", conv_launch(p, 2, std::min(p->conv_grid, nv * a.vsplit), st, a));
+      a.Vs = p->d_Vs;
+      a.T = p->d_P;
+      a.chunkY = cy;
+      a.nchunks = nc;
+      LAUNCH(p, K_CONV_ADJ, st, "k_conv_adj",
+             conv_launch(p, p->adj_stage ? 4 : 1, std::min(p->conv_grid, nv * nc), st, a, p->conv_smem_adj));
+    }
     dim3 grid(g.nz, nsplit);
     const size_t rsm = p->rota_smem_ok ? p->rota_smem : 0;
     if (p->interp == SPECT_INTERP_ONE) {
@@ -739,7 +808,7 @@ int static_scratch_address(void** out) {
 // projector for nv views on the plan's own buffers and keeps the fastest;
 // results are cached per plan shape for the process.
 struct TuneResult {
-  int fwd_cy, adj_cy, rotf_nsplit, nsplit_adj;
+  int fwd_cy, adj_cy, rotf_nsplit, nsplit_adj, sep, sep_adj;
   double fwd_ms, adj_ms;
 };
 std::mutex g_tune_mu;
@@ -748,7 +817,8 @@ std::vector<std::pair<std::string, TuneResult>> g_tune_cache;
 std::string tune_key(const spect_plan_s* p, int nv) {
   return std::to_string(p->nx) + "x" + std::to_string(p->nz) + "/" + std::to_string(p->px) + "x" +
          std::to_string(p->pz) + "/v" + std::to_string(p->nview) + "/n" + std::to_string(nv) + "/i" +
-         std::to_string(p->interp) + "/a" + std::to_string(p->d_att ? 1 : 0) + "/d" + std::to_string(p->device);
+         std::to_string(p->interp) + "/a" + std::to_string(p->d_att ? 1 : 0) + "/d" + std::to_string(p->device) +
+         "/s" + std::to_string(p->sep_fwd_ok) + std::to_string(p->sep_adj_ok) + std::to_string(p->sep_forced);
 }
 
 int time_pass(spect_plan_s* p, bool adj, int nv, int reps, double* ms) {
@@ -785,6 +855,8 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
         p->tune_adj_cy = kv.second.adj_cy;
         p->tune_rotf_nsplit = kv.second.rotf_nsplit;
         p->nsplit_adj = kv.second.nsplit_adj;
+        p->sep = kv.second.sep && p->sep_fwd_ok;
+        p->sep_adj = kv.second.sep_adj && p->sep_adj_ok;
         *fwd_ms = kv.second.fwd_ms;
         *adj_ms = kv.second.adj_ms;
         return SPECT_OK;
@@ -805,42 +877,58 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
     int c = best_chunk(p, nv, c0);
     if (std::find(cys.begin(), cys.end(), c) == cys.end()) cys.push_back(c);
   }
-  // forward: depth tile x rotation split
+  // convolution kernels to try: direct (separable planes) and FFT, unless
+  // SPECT_CONV fixed the choice
+  std::vector<int> fconv = {p->sep}, aconv = {p->sep_adj};
+  if (!p->sep_forced) {
+    if (p->sep_fwd_ok) fconv = {1, 0};
+    if (p->sep_adj_ok) aconv = {1, 0};
+  }
+  // forward: convolution kernel x depth tile x rotation split
   std::vector<int> rsplits = {0};
   for (int f : {1, 2, 4, 8})
     if (f * p->g.nz <= 8 * p->sm_count) rsplits.push_back(f);
   double bf = 1e300;
-  int bcy = cys[0], brs = 0, rc = SPECT_OK;
-  for (int cy : cys)
-    for (int rs : rsplits) {
-      p->tune_fwd_cy = cy;
-      p->tune_rotf_nsplit = rs;
-      double t;
-      if ((rc = time_pass(p, false, nv, 2, &t)) != SPECT_OK) break;
-      if (t < bf) {
-        bf = t;
-        bcy = cy;
-        brs = rs;
+  int bcy = cys[0], brs = 0, bsep = p->sep, rc = SPECT_OK;
+  for (int sp : fconv)
+    for (int cy : cys)
+      for (int rs : rsplits) {
+        if (rc != SPECT_OK) break;
+        p->sep = sp;
+        p->tune_fwd_cy = cy;
+        p->tune_rotf_nsplit = rs;
+        double t;
+        if ((rc = time_pass(p, false, nv, 2, &t)) != SPECT_OK) break;
+        if (t < bf) {
+          bf = t;
+          bcy = cy;
+          brs = rs;
+          bsep = sp;
+        }
       }
-    }
+  p->sep = bsep;
   p->tune_fwd_cy = bcy;
   p->tune_rotf_nsplit = brs;
-  // adjoint: depth tile x view split of the rotation adjoint
+  // adjoint: convolution kernel x depth tile x view split of the rotation adjoint
   double ba = 1e300;
-  int bacy = cys[0], bns = p->nsplit_adj;
-  for (int cy : cys)
-    for (int ns : {1, 2, 4, 8, 16}) {
-      if (rc != SPECT_OK || ns > p->nsplit_adj_max) break;
-      p->tune_adj_cy = cy;
-      p->nsplit_adj = ns;
-      double t;
-      if ((rc = time_pass(p, true, nv, 2, &t)) != SPECT_OK) break;
-      if (t < ba) {
-        ba = t;
-        bacy = cy;
-        bns = ns;
+  int bacy = cys[0], bns = p->nsplit_adj, basep = p->sep_adj;
+  for (int sp : aconv)
+    for (int cy : cys)
+      for (int ns : {1, 2, 4, 8, 16}) {
+        if (rc != SPECT_OK || ns > p->nsplit_adj_max) break;
+        p->sep_adj = sp;
+        p->tune_adj_cy = cy;
+        p->nsplit_adj = ns;
+        double t;
+        if ((rc = time_pass(p, true, nv, 2, &t)) != SPECT_OK) break;
+        if (t < ba) {
+          ba = t;
+          bacy = cy;
+          bns = ns;
+          basep = sp;
+        }
       }
-    }
+  p->sep_adj = basep;
   p->tune_adj_cy = bacy;
   p->nsplit_adj = bns;
   p->prof.on = prof;
@@ -848,7 +936,7 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
   *fwd_ms = bf;
   *adj_ms = ba;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache.push_back({key, TuneResult{bcy, bacy, brs, bns, bf, ba}});
+  g_tune_cache.push_back({key, TuneResult{bcy, bacy, brs, bns, bsep, basep, bf, ba}});
   return SPECT_OK;
 }
 
@@ -1269,6 +1357,107 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       return bail(SPECT_ERR_CUDA);
     }
   }
+  // separable PSF planes: factor every distinct stack's planes h = a b^T
+  {
+    const int zp = sep_zp(pz), xp = sep_xp(px), hs = zp + xp, hxs = (px - 1) / 2, hzs = (pz - 1) / 2;
+    const int ts = std::max(4, (2 * hxs + 2 * hzs + 3) & ~3);
+    std::vector<float> H((size_t)p->nset * ny * 2 * hs, 0.f), Tl((size_t)p->nset * ny * ts, 0.f);
+    bool ok = true;
+    std::vector<double> a(px), b(pz);
+    auto gauss_taps = [](int n, double fwhm, std::vector<double>& w) {
+      const int h = (n - 1) / 2;
+      if (fwhm == 0) {
+        for (int i = 0; i < n; ++i) w[i] = (i == h) ? 1.0 : 0.0;
+        return;
+      }
+      const double sigma = fwhm / std::sqrt(std::log(256.0));
+      double s = 0;
+      for (int i = 0; i < n; ++i) {
+        const double q = (double)(i - h) / sigma;
+        w[i] = std::exp(-0.5 * q * q);
+        s += w[i];
+      }
+      for (auto& v : w) v /= s;
+    };
+    for (int u = 0; u < p->nset && ok; ++u)
+      for (int y = 0; y < ny && ok; ++y) {
+        if (opts.gauss) {
+          auto fw = [&](double f0, double f1) {
+            return ny <= 1 ? f0 : (y == ny - 1 ? f1 : f0 + y * ((f1 - f0) / (ny - 1)));
+          };
+          gauss_taps(px, fw(opts.gx0, opts.gx1), a);
+          gauss_taps(pz, fw(opts.gz0, opts.gz1), b);
+        } else {
+          const float* k = psfs + ((size_t)uniq[u] * ny + y) * pp;  // k[i + px j]
+          const int i0 = (px - 1) / 2, j0 = (pz - 1) / 2;
+          const double c = k[i0 + (size_t)px * j0];
+          double mx = 0;
+          for (size_t e = 0; e < pp; ++e) mx = std::max(mx, (double)std::fabs(k[e]));
+          if (!(c != 0.0) || !(mx > 0.0)) {
+            ok = false;
+            break;
+          }
+          for (int i = 0; i < px; ++i) a[i] = k[i + (size_t)px * j0];
+          for (int j = 0; j < pz; ++j) b[j] = k[i0 + (size_t)px * j] / c;
+          double res = 0;
+          for (int j = 0; j < pz; ++j)
+            for (int i = 0; i < px; ++i) res = std::max(res, std::fabs(k[i + (size_t)px * j] - a[i] * b[j]));
+          if (res > 1e-6 * mx) {
+            ok = false;
+            break;
+          }
+        }
+        // [wz reversed | wx reversed | b | a], each zero-padded (zp, xp)
+        float* hrow = H.data() + ((size_t)u * ny + y) * 2 * hs;
+        for (int m = 0; m < pz; ++m) hrow[m] = (float)b[pz - 1 - m];
+        for (int m = 0; m < px; ++m) hrow[zp + m] = (float)a[px - 1 - m];
+        for (int m = 0; m < pz; ++m) hrow[hs + m] = (float)b[m];
+        for (int m = 0; m < px; ++m) hrow[hs + zp + m] = (float)a[m];
+        // adjoint edge tails: cL_k = sum_{d>k} w(d), cR_k = sum_{d<-k} w(d)
+        float* trow = Tl.data() + ((size_t)u * ny + y) * ts;
+        auto tails = [](const std::vector<double>& w, int h, float* L, float* R) {
+          for (int k = 0; k < h; ++k) {
+            double l = 0, r = 0;
+            for (int i = h + k + 1; i <= 2 * h; ++i) l += w[i];
+            for (int i = 0; i < h - k; ++i) r += w[i];
+            L[k] = (float)l;
+            R[k] = (float)r;
+          }
+        };
+        tails(a, hxs, trow, trow + hxs);
+        tails(b, hzs, trow + 2 * hxs, trow + 2 * hxs + hzs);
+      }
+    if (ok) {
+      if ((st = dalloc(p, &p->d_Hsep, H.size())) || (st = up(p->d_Hsep, H.data(), sizeof(float) * H.size())) ||
+          (st = dalloc(p, &p->d_Tsep, Tl.size())) || (st = up(p->d_Tsep, Tl.data(), sizeof(float) * Tl.size())))
+        return bail(st);
+      p->sep_ok = 1;
+      p->sep_hs = hs;
+      p->sep_ts = ts;
+      const int att = (p->d_att && interpmeth == SPECT_INTERP_TWO) ? 1 : 0;
+      p->sep_fwd_smem = sconv_fwd_smem(nx, nz, px, pz, att);
+      // SPECT_CONV=fft: FFT kernels only; SPECT_CONV=direct: direct kernels
+      // wherever they run (neither is then re-chosen by the autotuner)
+      const char* cm = std::getenv("SPECT_CONV");
+      const bool only_fft = cm && std::strcmp(cm, "fft") == 0;
+      p->sep_forced = only_fft ? 1 : (cm && std::strcmp(cm, "direct") == 0) ? 2 : 0;
+      p->sep_shape_fwd = nx % kSepXB == 0 ? sep_pick_shape(nx, nz, px, pz, true) : -1;
+      p->sep_shape_adj = nx % kSepXB == 0 ? sep_pick_shape(nx, nz, px, pz, false) : -1;
+      p->sep_fwd_ok = (p->sep_shape_fwd >= 0 && p->sep_fwd_smem <= p->max_smem) ? 1 : 0;
+      p->sep = p->sep_fwd_ok && !only_fft;
+      if (p->sep_fwd_ok)
+        CUDA_TRY(cudaFuncSetAttribute(kSconvFwd[p->sep_shape_fwd], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)p->max_smem));
+      // adjoint: multiplies the attenuation exactly when the rotation adjoint
+      // expects premultiplied planes (adj_stage)
+      p->sep_adj_smem = sconv_adj_smem(nx, nz, px, pz, ts, p->adj_stage ? 1 : 0);
+      p->sep_adj_ok = (p->sep_shape_adj >= 0 && p->sep_adj_smem <= p->max_smem) ? 1 : 0;
+      p->sep_adj = p->sep_adj_ok && !only_fft;
+      if (p->sep_adj_ok)
+        CUDA_TRY(cudaFuncSetAttribute(kSconvAdj[p->sep_shape_adj], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)p->max_smem));
+    }
+  }
   *out = p;
   return SPECT_OK;
 }
@@ -1295,6 +1484,16 @@ int spect_plan_info(spect_plan_t p, int out[8], size_t* bytes) {
   int v[8] = {p->nx, p->ny, p->nz, p->px, p->pz, p->nview, p->interp, p->nset};
   std::memcpy(out, v, sizeof(v));
   if (bytes) *bytes = p->bytes;
+  return SPECT_OK;
+}
+
+int spect_plan_conv_kernels(spect_plan_t p, int out[4]) {
+  if (!p || !out) return fail(SPECT_ERR_ARG, "null pointer argument");
+  std::lock_guard<std::mutex> lk(p->mu);
+  out[0] = p->sep_fwd_ok;
+  out[1] = p->sep_adj_ok;
+  out[2] = p->sep;
+  out[3] = p->sep_adj;
   return SPECT_OK;
 }
 

@@ -48,3 +48,68 @@ def test_plan_from_device_psfs(S, O):
     assert relerr(v1, G.project(x)) <= 1e-4
     gp.close()
     ref.close()
+
+
+def test_separable_matches_fft_path(S, O, monkeypatch):
+    """Gaussian (rank-1) PSF planes take the direct separable convolution;
+    SPECT_CONV=fft forces the FFT kernels.  Both must agree with each other and
+    with the oracle (which convolves with the full 2-D kernel)."""
+    import importlib
+
+    W = importlib.import_module("spectrecon_b200.workloads")
+    st = W.make_study("t", nx=128, nz=80, nview=24, p=37, fwhm_end=6.0, k=6, mu_values=(0.0096, 0.015),
+                      nblocks=1, niter=1, seed=3)
+    idx = np.array([0, 5, 11, 23], np.int32)
+    sep = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    monkeypatch.setenv("SPECT_CONV", "fft")
+    fft = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    monkeypatch.delenv("SPECT_CONV")
+    assert sep.conv_kernels() == {"forward": "direct", "adjoint": "direct", "direct_forward_ok": True,
+                                  "direct_adjoint_ok": True}
+    assert fft.conv_kernels() == {"forward": "fft", "adjoint": "fft", "direct_forward_ok": True,
+                                  "direct_adjoint_ok": True}
+    v_sep, v_fft = S.project(st.image, sep, index=idx), S.project(st.image, fft, index=idx)
+    assert relerr(v_sep, v_fft) <= 1e-5
+    G64 = O.Geometry(st.mumap, st.psfs, st.dy, dtype=np.float64)
+    assert relerr(v_sep, G64.project(st.image, index=idx)) <= 1e-4
+    rng = np.random.default_rng(4)
+    y = np.asfortranarray(rng.random((128, 80, idx.size)), np.float32)
+    b_sep, b_fft = S.backproject(y, sep, index=idx), S.backproject(y, fft, index=idx)
+    assert relerr(b_sep, b_fft) <= 1e-5
+    assert relerr(b_sep, G64.backproject(y, index=idx)) <= 1e-4
+    sep.close()
+    fft.close()
+
+
+@pytest.mark.gpu
+def test_autotune_convolution_choice(S, O):
+    """autotune() keeps the faster of the direct and FFT convolution per
+    direction; whatever it keeps, results stay within tolerance of the oracle.
+    Non-separable PSF planes never get the direct kernels."""
+    import importlib
+
+    W = importlib.import_module("spectrecon_b200.workloads")
+    st = W.make_study("t", nx=64, nz=48, nview=16, p=17, fwhm_end=4.0, k=4, mu_values=(0.0096, 0.015),
+                      nblocks=2, niter=1, seed=5)
+    plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    plan.autotune(8)
+    ck = plan.conv_kernels()
+    assert ck["direct_forward_ok"] and ck["direct_adjoint_ok"]
+    assert ck["forward"] in ("direct", "fft") and ck["adjoint"] in ("direct", "fft")
+    G64 = O.Geometry(st.mumap, st.psfs, st.dy, dtype=np.float64)
+    idx = np.arange(0, 16, 2, dtype=np.int32)
+    assert relerr(S.project(st.image, plan, index=idx), G64.project(st.image, index=idx)) <= 1e-4
+    y = np.asfortranarray(np.random.default_rng(6).random((64, 48, idx.size)), np.float32)
+    assert relerr(S.backproject(y, plan, index=idx), G64.backproject(y, index=idx)) <= 1e-4
+    plan.close()
+    # rank-2 planes g1 g2' + g2 g1' (two Gaussian widths) are not separable
+    px, pz, ny = st.psfs.shape[:3]
+    gx1, gx2 = (np.exp(-(np.arange(px) - px // 2) ** 2 / (2 * s * s)) for s in (1.0, 3.0))
+    gz1, gz2 = (np.exp(-(np.arange(pz) - pz // 2) ** 2 / (2 * s * s)) for s in (1.0, 3.0))
+    plane = np.outer(gx1, gz2) + np.outer(gx2, gz1)
+    psfs = np.asfortranarray(np.repeat((plane / plane.sum())[:, :, None], ny, axis=2), np.float32)  # (px, pz, ny)
+    q = S.SPECTplan(st.mumap, psfs, st.dy)
+    assert q.conv_kernels()["forward"] == "fft" and q.conv_kernels()["adjoint"] == "fft"
+    q.autotune(8)
+    assert q.conv_kernels()["forward"] == "fft" and q.conv_kernels()["adjoint"] == "fft"
+    q.close()
