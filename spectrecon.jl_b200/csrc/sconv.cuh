@@ -32,17 +32,18 @@
 
 namespace spect {
 
-constexpr int kSepZB = 8;     // z outputs per z-pass task
-constexpr int kSepXB = 4;     // x outputs per x-pass task
+constexpr int kSepZB = 8;  // z outputs per z-pass task
+constexpr int kSepXB = 8;  // x outputs per x-pass task
 
 // launch shapes: NT x-pass tasks per thread, NTH threads per block (one block
-// per SM; 640 threads leave at most 102 registers a thread, enough for NT <= 4)
+// per SM; 640 threads leave at most 102 registers a thread, 1024 threads 64:
+// each NT here runs without spills)
 struct SepShape {
   int nt, nth;
 };
-constexpr int kSepNShapes = 10;
-constexpr SepShape kSepShapes[kSepNShapes] = {{1, 512}, {2, 512}, {3, 512}, {4, 512}, {5, 512},
-                                              {6, 512}, {1, 640}, {2, 640}, {3, 640}, {4, 640}};
+constexpr int kSepNShapes = 9;
+constexpr SepShape kSepShapes[kSepNShapes] = {{1, 512}, {2, 512}, {3, 512}, {4, 512}, {1, 640},
+                                              {2, 640}, {3, 640}, {1, 1024}, {2, 1024}};
 
 __host__ __device__ constexpr int sep_zp(int pz) { return (pz + kSepZB - 1) / kSepZB * kSepZB; }
 __host__ __device__ constexpr int sep_xp(int px) { return (px + kSepXB - 1) / kSepXB * kSepXB; }
@@ -55,8 +56,9 @@ __host__ __device__ constexpr int sep_bs(int nx, int px) { return (nx + sep_xp(p
 
 // the launch shape (index into kSepShapes) with the least FMA work per plane
 // summed over the block's thread slots, tasks padded to whole lock-step
-// groups; resident: every x task of the block fits at once (the forward keeps
-// its x-pass outputs in registers across a depth chunk); -1 if none fits
+// groups (ties: the later shape, more tasks a thread); resident: every x task
+// of the block fits at once (the forward keeps its x-pass outputs in
+// registers across a depth chunk); -1 if none fits
 inline int sep_pick_shape(int nx, int nz, int px, int pz, bool resident) {
   const int xtasks = nz * (nx / kSepXB), ztasks = nx * ((nz + kSepZB - 1) / kSepZB);
   int best = -1;
@@ -66,7 +68,7 @@ inline int sep_pick_shape(int nx, int nz, int px, int pz, bool resident) {
     if (resident && nt * nth < xtasks) continue;
     const double xr = (xtasks + nt * nth - 1) / (nt * nth), zr = (ztasks + nzt * nth - 1) / (nzt * nth);
     const double c = (double)nth * (xr * nt * kSepXB * sep_xp(px) + zr * nzt * kSepZB * sep_zp(pz));
-    if (best < 0 || c < bc) {
+    if (best < 0 || c <= bc) {
       best = i;
       bc = c;
     }
@@ -273,8 +275,10 @@ __global__ void __launch_bounds__(NTH, 1) k_sconv_fwd(SepArgs a) {
 #pragma unroll
     for (int i = 0; i < NT; ++i)
       if ((int)threadIdx.x + i * NTH < xtasks)
-        *reinterpret_cast<float4*>(out + (size_t)xz[i] * nx + xx[i]) =
-            make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+#pragma unroll
+        for (int q = 0; q < kSepXB / 4; ++q)
+          *reinterpret_cast<float4*>(out + (size_t)xz[i] * nx + xx[i] + 4 * q) =
+              make_float4(acc[i][4 * q], acc[i][4 * q + 1], acc[i][4 * q + 2], acc[i][4 * q + 3]);
   }
 }
 

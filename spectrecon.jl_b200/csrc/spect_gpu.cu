@@ -478,8 +478,8 @@ Conv2Args conv_args(const spect_plan_s* p) {
 // k_sconv_fwd / k_sconv_adj instantiations, in kSepShapes order
 #define SEP_SHAPES(K)                                                                                   \
   {(const void*)K<1, 512>, (const void*)K<2, 512>, (const void*)K<3, 512>, (const void*)K<4, 512>,   \
-   (const void*)K<5, 512>, (const void*)K<6, 512>, (const void*)K<1, 640>, (const void*)K<2, 640>,   \
-   (const void*)K<3, 640>, (const void*)K<4, 640>}
+   (const void*)K<1, 640>, (const void*)K<2, 640>, (const void*)K<3, 640>, (const void*)K<1, 1024>,  \
+   (const void*)K<2, 1024>}
 const void* const kSconvFwd[kSepNShapes] = SEP_SHAPES(k_sconv_fwd);
 const void* const kSconvAdj[kSepNShapes] = SEP_SHAPES(k_sconv_adj);
 #undef SEP_SHAPES

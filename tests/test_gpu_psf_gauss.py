@@ -103,11 +103,12 @@ def test_autotune_convolution_choice(S, O):
     assert relerr(S.backproject(y, plan, index=idx), G64.backproject(y, index=idx)) <= 1e-4
     plan.close()
     # rank-2 planes g1 g2' + g2 g1' (two Gaussian widths) are not separable
-    px, pz, ny = st.psfs.shape[:3]
+    px, pz, ny, nview = st.psfs.shape
     gx1, gx2 = (np.exp(-(np.arange(px) - px // 2) ** 2 / (2 * s * s)) for s in (1.0, 3.0))
     gz1, gz2 = (np.exp(-(np.arange(pz) - pz // 2) ** 2 / (2 * s * s)) for s in (1.0, 3.0))
     plane = np.outer(gx1, gz2) + np.outer(gx2, gz1)
-    psfs = np.asfortranarray(np.repeat((plane / plane.sum())[:, :, None], ny, axis=2), np.float32)  # (px, pz, ny)
+    psfs = np.asfortranarray(np.broadcast_to((plane / plane.sum())[:, :, None, None], (px, pz, ny, nview)),
+                             np.float32)
     q = S.SPECTplan(st.mumap, psfs, st.dy)
     assert q.conv_kernels()["forward"] == "fft" and q.conv_kernels()["adjoint"] == "fft"
     q.autotune(8)
