@@ -280,6 +280,8 @@ def run_ours(args):
                 "convolution": conv["forward" if dom == "k_conv_fwd" else "adjoint"],
                 "peak_source": "measured cuBLAS SGEMM (TF32 off) in this run",
                 "flops_per_launch": flops_launch, "avg_launch_ms": round(avg_ms, 4),
+                # DRAM bytes of one launch (ncu capture in profiles/) over its live duration
+                "hbm_gbs": round(traffic / (avg_ms / 1e3) / 1e9, 1) if traffic and avg_ms > 0 else None,
                 "kernel_ms_per_step": {k: round(v / args.steps, 3) for k, v in kms.items()},
                 "kernel_launches_per_step": {k: int(v // args.steps) for k, v in kn.items()}}
     batched = served = None
