@@ -153,7 +153,7 @@ def build_study(S, plan_factory):
         plan.close()
         return v
 
-    return W.config_study("c2", project_fn=proj)
+    return W.named_study("larger_128x128x80", project_fn=proj)
 
 
 def run_ours(args):
@@ -352,7 +352,7 @@ def run_batched(S, torch, njobs=32, timed_runs=2, plain_sample=6, seed=3):
     jobs = W.batch_mix(njobs, seed)
     plans, studies = [], []
     for j in jobs:
-        st = W.make_study("c3", nx=j["nx"], nz=j["nz"], nview=j["nview"], p=j["p"], fwhm_end=j["fwhm_end"],
+        st = W.make_study("batch_job", nx=j["nx"], nz=j["nz"], nview=j["nview"], p=j["p"], fwhm_end=j["fwhm_end"],
                           k=j["k"], mu_values=j["mu_values"], nblocks=j["nblocks"], niter=j["niter"], seed=j["seed"],
                           project_fn=lambda im, s: S.project(im, S.SPECTplan(s.mumap, s.psfs, s.dy)))
         plans.append(S.SPECTplan(st.mumap, st.psfs, st.dy))
@@ -419,7 +419,7 @@ def run_served(S, njobs=500, rate=10.0, big_fraction=0.1, seed=4, pool_small=36,
         b["nblocks"] = int(rng.choice(W.divisors_in(b["nview"])))
     pool = []
     for j in mix + big:
-        st = W.make_study("c4", nx=j["nx"], nz=j["nz"], nview=j["nview"], p=j["p"], fwhm_end=j["fwhm_end"],
+        st = W.make_study("served_job", nx=j["nx"], nz=j["nz"], nview=j["nview"], p=j["p"], fwhm_end=j["fwhm_end"],
                           k=j["k"], mu_values=j["mu_values"], nblocks=j["nblocks"], niter=j["niter"], seed=j["seed"])
         plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
         ytrue = S.project(st.image, plan).astype(np.float64)
@@ -548,7 +548,7 @@ def run_reference(args):
     from importlib import import_module
 
     W = import_module("spectrecon_b200.workloads")
-    st = W.config_study("c2", project_fn=proj)
+    st = W.named_study("larger_128x128x80", project_fn=proj)
     for _ in range(args.warmup):
         pass  # the oracle has no warm-up state
     vals = []

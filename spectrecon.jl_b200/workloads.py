@@ -1,7 +1,7 @@
 """Seeded synthetic SPECT studies (no public dataset exists for this path).
 
 Each study follows the shapes and value distributions of the benchmark
-configurations: ellipsoid emission phantoms (background 0.1 inside the
+workloads: ellipsoid emission phantoms (background 0.1 inside the
 field of view, intensities U[0.5, 2]), ellipsoid attenuation maps in 1/mm
 for a 4.8 mm voxel (0.0096/mm = 0.096/cm soft tissue, 0.015/mm = 0.15/cm,
 0.004/mm lung-like), depth-dependent Gaussian PSFs from ``psf_gauss``
@@ -107,20 +107,23 @@ def make_study(name, nx, nz, nview, p, fwhm_end, k, mu_values, nblocks, niter, s
     return st
 
 
-# The five benchmark configurations (sizes, PSFs, attenuation, EM schedule).
-CONFIGS = {
-    "c1": dict(nx=64, nz=64, nview=64, p=11, fwhm_end=3.0, k=4, mu_values=(0.0096,), nblocks=1, niter=16),
-    "c2": dict(nx=128, nz=80, nview=120, p=37, fwhm_end=6.0, k=8, mu_values=(0.0096, 0.015), nblocks=8, niter=4,
-               counts=1e6),
-    "c5": dict(nx=256, nz=200, nview=128, p=65, fwhm_end=10.0, k=12, mu_values=(0.0096, 0.015, 0.004),
-               nblocks=16, niter=4),
+# Named studies (sizes, PSFs, attenuation, EM schedule) with their fixed seeds.
+STUDIES = {
+    "small_64x64x64": dict(nx=64, nz=64, nview=64, p=11, fwhm_end=3.0, k=4, mu_values=(0.0096,), nblocks=1,
+                           niter=16),
+    "larger_128x128x80": dict(nx=128, nz=80, nview=120, p=37, fwhm_end=6.0, k=8, mu_values=(0.0096, 0.015),
+                              nblocks=8, niter=4, counts=1e6),
+    "large_256x256x200": dict(nx=256, nz=200, nview=128, p=65, fwhm_end=10.0, k=12,
+                              mu_values=(0.0096, 0.015, 0.004), nblocks=16, niter=4),
 }
+STUDY_SEED_OFFSET = {"small_64x64x64": 0, "larger_128x128x80": 1, "large_256x256x200": 4}
 
 
-def config_study(name, project_fn=None, seed_offset=0):
-    cfg = dict(CONFIGS[name])
-    idx = {"c1": 0, "c2": 1, "c5": 4}[name]
-    return make_study(name, seed=BASE_SEED + idx + seed_offset, project_fn=project_fn, **cfg)
+def named_study(name, project_fn=None, seed_offset=0):
+    """The named study of STUDIES, generated from its fixed seed."""
+    cfg = dict(STUDIES[name])
+    return make_study(name, seed=BASE_SEED + STUDY_SEED_OFFSET[name] + seed_offset, project_fn=project_fn,
+                      **cfg)
 
 
 def divisors_in(n, lo=4, hi=16):
@@ -128,7 +131,7 @@ def divisors_in(n, lo=4, hi=16):
 
 
 def batch_mix(njobs, seed, big_fraction=0.0):
-    """Uneven job mix of the batching/serving configurations: nx=ny in
+    """Uneven job mix of the batching/serving workloads: nx=ny in
     {64,96,128}, nz in [48,128], views in {60,90,120,128}, PSF in {11,21,37}
     (FWHM 1 -> p/6), OS-EM subsets from the divisors of nview in [4,16], and
     optionally a fraction of 256x256x128 jobs."""

@@ -1,4 +1,4 @@
-"""GPU parity at the benchmark configurations' padded sizes (C ABI vs oracle).
+"""GPU parity at the benchmark workloads' padded sizes (C ABI vs oracle).
 
 Covers every code path of the convolution kernels: register accumulators
 (256x128, 128x128 padded planes), global accumulator slabs (256x256,
@@ -22,10 +22,10 @@ def _study(S, nx, nz, nview, p, fwhm_end, mu_values, seed):
                         nblocks=1, niter=1, seed=seed)
 
 @pytest.mark.parametrize("nx,nz,nview,p,fwhm,idx", [
-    (64, 64, 64, 11, 3.0, [0, 5, 16, 31, 47]),            # C1 sizes: 128x128 padded
-    (128, 80, 120, 37, 6.0, [0, 7, 30, 61, 119]),          # C2 sizes: 256x128 padded
-    (128, 128, 60, 37, 6.0, [3, 29]),                      # C3 largest: 256x256 padded (global slabs)
-    (96, 48, 90, 21, 3.5, [0, 44, 89]),                    # C3 mid: 128x128 padded, nx = 96
+    (64, 64, 64, 11, 3.0, [0, 5, 16, 31, 47]),            # 64x64x64, 11x11 PSF: 128x128 padded
+    (128, 80, 120, 37, 6.0, [0, 7, 30, 61, 119]),          # 128x128x80, 37x37 PSF: 256x128 padded
+    (128, 128, 60, 37, 6.0, [3, 29]),                      # 128x128x128, 37x37 PSF: 256x256 padded (global slabs)
+    (96, 48, 90, 21, 3.5, [0, 44, 89]),                    # 96x96x48, 21x21 PSF: 128x128 padded
 ])
 def test_config_parity(S, O, nx, nz, nview, p, fwhm, idx):
     st = _study(S, nx, nz, nview, p, fwhm, (0.0096, 0.015), seed=nx + nz + p)
@@ -43,7 +43,7 @@ def test_config_parity(S, O, nx, nz, nview, p, fwhm, idx):
     assert relerr(b, G64.backproject(y, index=idx)) <= TOL
 
 def test_large_512_planes(S, O):
-    """C5-class plane: 256x256x200 image, 65x65 PSF -> 512x512 padded planes.
+    """Largest plane: 256x256x200 image, 65x65 PSF -> 512x512 padded planes.
 
     At this size the reference's own Float32 adjoint carries ~1.8e-4 of FFT
     round-off (fft_conv_adj! sums all 128+156 padded rows/columns into the edge
@@ -70,7 +70,7 @@ def test_full_c2_subset_osem_update(S, O):
     """One OS-EM iteration (8 subsets of 15 views) of the benchmark study vs the oracle."""
     import importlib
     W = importlib.import_module("spectrecon_b200.workloads")
-    st = W.config_study("c2", project_fn=lambda im, s: O.Geometry(s.mumap, s.psfs, s.dy).project(im))
+    st = W.named_study("larger_128x128x80", project_fn=lambda im, s: O.Geometry(s.mumap, s.psfs, s.dy).project(im))
     plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
     G = O.Geometry(st.mumap, st.psfs, st.dy)
     x0 = np.ones(st.image.shape, np.float32, order="F")

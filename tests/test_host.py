@@ -103,8 +103,8 @@ def test_em_background_check(S):
 def test_workloads_seeded(S):
     import importlib
     W = importlib.import_module("spectrecon_b200.workloads")
-    a = W.config_study("c1")
-    b = W.config_study("c1")
+    a = W.named_study("small_64x64x64")
+    b = W.named_study("small_64x64x64")
     assert np.array_equal(a.image, b.image) and np.array_equal(a.mumap, b.mumap)
     assert a.image.shape == (64, 64, 64) and a.psfs.shape == (11, 11, 64, 64)
     assert a.image.min() >= 0 and 0.5 < a.image.max() <= 2.1 + 12 * 2
