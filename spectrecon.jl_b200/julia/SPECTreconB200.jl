@@ -17,7 +17,7 @@
 module SPECTreconB200
 
 export SPECTplan, project, project!, backproject, backproject!
-export mlem, mlem!, osem, osem!, Ablock, psf_gauss
+export mlem, mlem!, osem, osem!, Ablock, psf_gauss, autotune!, conv_kernels
 
 const LIB = get(ENV, "SPECT_B200_LIB", joinpath(@__DIR__, "..", "libspectgpu.so"))
 
@@ -219,6 +219,31 @@ function psf_gauss( ; ny::Int = 128, px::Int = 11, pz::Int = px, fwhm_start::Rea
     check(ccall((:spect_psf_gauss, LIB), Cint, (Ptr{Float32}, Cint, Cint, Cint, Ptr{Float64}, Ptr{Float64}),
         psf, ny, px, pz, Vector{Float64}(fwhm_x), Vector{Float64}(fwhm_z)))
     return T.(psf)
+end
+
+# ---- additions without a counterpart in the reference ------------------------
+
+"""
+    autotune!(plan; nindex = plan.nview) -> (forward_ms, adjoint_ms)
+Times the launch shapes and, for rank-1 (Gaussian) PSF planes, the direct
+separable convolution against the FFT one for calls of `nindex` views, and
+keeps the fastest per direction.
+"""
+function autotune!(plan::SPECTplan; nindex::Int = plan.nview)
+    ms = zeros(Float64, 2)
+    check(ccall((:spect_plan_autotune, LIB), Cint, (Ptr{Cvoid}, Cint, Ptr{Float64}), plan.handle, nindex, ms))
+    return (ms[1], ms[2])
+end
+
+"""
+    conv_kernels(plan) -> (forward = :direct | :fft, adjoint = :direct | :fft)
+Which PSF convolution each direction of the plan runs.
+"""
+function conv_kernels(plan::SPECTplan)
+    out = zeros(Cint, 4)
+    check(ccall((:spect_plan_conv_kernels, LIB), Cint, (Ptr{Cvoid}, Ptr{Cint}), plan.handle, out))
+    name(k) = k == 1 ? :direct : :fft
+    return (forward = name(out[3]), adjoint = name(out[4]))
 end
 
 end # module
