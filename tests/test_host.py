@@ -27,6 +27,15 @@ def test_library_exports_every_header_symbol(S):
     assert set(names) <= set(S._native.symbols())
 
 
+def test_julia_shim_binds_declared_symbols():
+    """Every ccall of the Julia shim names a function that include/spect_gpu.h
+    declares (the shim cannot run here: no Julia)."""
+    src = open(os.path.join(ROOT, "spectrecon.jl_b200", "julia", "SPECTreconB200.jl")).read()
+    called = set(re.findall(r"ccall\(\(:(spect_\w+),", src))
+    assert {"spect_plan_create", "spect_project_host", "spect_backproject_host", "spect_osem_host"} <= called
+    assert called <= set(header_functions()), called - set(header_functions())
+
+
 def test_build_targets_sm100a():
     import __graft_entry__ as GE
     assert "arch=compute_100a,code=sm_100a" in GE.NVCC_FLAGS
