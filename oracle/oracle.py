@@ -140,6 +140,35 @@ class Geometry:
         return out
 
 
+def psf_gauss(ny=128, px=11, pz=None, fwhm_start=1.0, fwhm_end=4.0, fwhm=None, fwhm_x=None, fwhm_z=None,
+              dtype=np.float32):
+    """psf_gauss(; ny, px, pz, fwhm_start, fwhm_end, fwhm, fwhm_x, fwhm_z, T)
+    restated in numpy (src/psf-gauss.jl:24-55): plane iy is the Float64
+    outer product of two normalised 1-D Gaussians exp(-0.5 (r/sigma)^2),
+    sigma = fwhm/sqrt(log 256), r = -(p-1)/2 .. (p-1)/2, rounded to T;
+    fwhm == 0 gives the Kronecker impulse at r == 0.  fwhm defaults to
+    range(fwhm_start, fwhm_end, ny) (numpy.linspace: same endpoints)."""
+    pz = px if pz is None else pz
+    if fwhm is None:
+        fwhm = np.linspace(fwhm_start, fwhm_end, ny)
+    fx = np.asarray(fwhm if fwhm_x is None else fwhm_x, dtype=np.float64)
+    fz = np.asarray(fx if fwhm_z is None else fwhm_z, dtype=np.float64)
+
+    def g(p, f):
+        r = np.arange(-(p - 1) // 2, (p - 1) // 2 + 1, dtype=np.float64)
+        if f == 0:
+            if not (r == 0).any():
+                raise ValueError("must have some r=0 if fwhm=0")
+            return (r == 0).astype(np.float64)
+        w = np.exp(-0.5 * (r / (f / np.sqrt(np.log(256.0)))) ** 2)
+        return w / w.sum()
+
+    out = np.empty((px, pz, ny), dtype=dtype, order="F")
+    for iy in range(ny):
+        out[:, :, iy] = np.outer(g(px, fx[iy]), g(pz, fz[iy])).astype(dtype)
+    return out
+
+
 def imrotate(img, theta, method="two", adj=False, dtype=np.float32):
     sfx, dt = _dt(dtype)
     img = _c(img, dt)

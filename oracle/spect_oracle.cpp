@@ -131,26 +131,69 @@ struct FFT1 {
   }
 };
 
-// 2-D DFT of an n1 x n2 column-major complex array (split re/im).
+// The DFT of FFT1 applied to every line along dim 2 of an m x n column-major
+// split array (line i = entries i, i + m, ...), all m lines at once: the same
+// bit reversal, butterflies and twiddles as FFT1::run, so each line's result
+// is bit-identical to FFT1::run on that line; the inner loop runs over the
+// contiguous dim 1 (vectorisable, unit stride).
+template <class T>
+void dft_along2(T* re, T* im, int m, const FFT1<T>& f, bool inverse) {
+  const int n = f.n;
+  for (int j = 0; j < n; ++j) {
+    const int r = f.rev[j];
+    if (r > j) {
+      std::swap_ranges(re + (size_t)j * m, re + (size_t)(j + 1) * m, re + (size_t)r * m);
+      std::swap_ranges(im + (size_t)j * m, im + (size_t)(j + 1) * m, im + (size_t)r * m);
+    }
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    const int half = len / 2, step = n / len;
+    for (int s = 0; s < n; s += len)
+      for (int k = 0; k < half; ++k) {
+        const T c = f.wr[k * step], d = inverse ? -f.wi[k * step] : f.wi[k * step];
+        T* __restrict ra = re + (size_t)(s + k) * m;
+        T* __restrict ia = im + (size_t)(s + k) * m;
+        T* __restrict rb = re + (size_t)(s + k + half) * m;
+        T* __restrict ib = im + (size_t)(s + k + half) * m;
+        for (int i = 0; i < m; ++i) {
+          const T xr = rb[i] * c - ib[i] * d;
+          const T xi = rb[i] * d + ib[i] * c;
+          rb[i] = ra[i] - xr;
+          ib[i] = ia[i] - xi;
+          ra[i] = ra[i] + xr;
+          ia[i] = ia[i] + xi;
+        }
+      }
+  }
+}
+
+// dst (n2 x n1) = transpose of src (n1 x n2), column-major, in cache tiles
+template <class T>
+void transpose_cm(T* __restrict dst, const T* __restrict src, int n1, int n2) {
+  constexpr int B = 16;
+  for (int j0 = 0; j0 < n2; j0 += B)
+    for (int i0 = 0; i0 < n1; i0 += B)
+      for (int j = j0; j < std::min(n2, j0 + B); ++j)
+        for (int i = i0; i < std::min(n1, i0 + B); ++i) dst[j + (size_t)i * n2] = src[i + (size_t)j * n1];
+}
+
+// 2-D DFT of an n1 x n2 column-major complex array (split re/im): the 1-D
+// DFT along dim 1 of every column, then along dim 2 of every row (each line
+// exactly FFT1::run).  Dim 1 runs on a transposed copy so that both passes
+// sweep contiguous memory.
 template <class T>
 struct FFT2 {
   int n1, n2;
   FFT1<T> f1, f2;
   std::vector<T> tr, ti;
-  FFT2(int a, int b) : n1(a), n2(b), f1(a), f2(b), tr(b), ti(b) {}
+  FFT2(int a, int b) : n1(a), n2(b), f1(a), f2(b), tr((size_t)a * b), ti((size_t)a * b) {}
   void run(T* re, T* im, bool inverse) {
-    for (int j = 0; j < n2; ++j) f1.run(re + (size_t)j * n1, im + (size_t)j * n1, inverse);
-    for (int i = 0; i < n1; ++i) {
-      for (int j = 0; j < n2; ++j) {
-        tr[j] = re[i + (size_t)j * n1];
-        ti[j] = im[i + (size_t)j * n1];
-      }
-      f2.run(tr.data(), ti.data(), inverse);
-      for (int j = 0; j < n2; ++j) {
-        re[i + (size_t)j * n1] = tr[j];
-        im[i + (size_t)j * n1] = ti[j];
-      }
-    }
+    transpose_cm(tr.data(), re, n1, n2);
+    transpose_cm(ti.data(), im, n1, n2);
+    dft_along2(tr.data(), ti.data(), n2, f1, inverse);
+    transpose_cm(re, tr.data(), n2, n1);
+    transpose_cm(im, ti.data(), n2, n1);
+    dft_along2(re, im, n1, f2, inverse);
     if (inverse) {  // AbstractFFTs ScaledPlan: multiply by 1/N
       T s = (T)(1.0 / ((double)n1 * n2));
       size_t N = (size_t)n1 * n2;
@@ -198,9 +241,12 @@ struct PsfWork {
     }
     fft.run(ir.data(), ii.data(), true);
     int m = Npx / 2, n = Npz / 2;  // fftshift2!: dst[i,j] = src[(i+m)%Npx, (j+n)%Npz]
-    for (int j = 0; j < Npz; ++j)
-      for (int i = 0; i < Npx; ++i)
-        work[i + (size_t)j * Npx] = ir[(i + m) % Npx + (size_t)((j + n) % Npz) * Npx];
+    for (int j = 0; j < Npz; ++j) {
+      const T* src = ir.data() + (size_t)((j + n) % Npz) * Npx;
+      T* dst = work.data() + (size_t)j * Npx;
+      for (int i = 0; i < Npx - m; ++i) dst[i] = src[i + m];
+      for (int i = Npx - m; i < Npx; ++i) dst[i] = src[i + m - Npx];
+    }
   }
 };
 

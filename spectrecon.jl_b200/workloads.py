@@ -79,16 +79,20 @@ class Study:
 
 
 def make_study(name, nx, nz, nview, p, fwhm_end, k, mu_values, nblocks, niter, seed, counts=None,
-               project_fn=None, fwhm_start=1.0):
+               project_fn=None, fwhm_start=1.0, psf_fn=None):
     """Build a study; ``project_fn(image, study) -> views`` supplies the
-    noiseless data (the GPU projector or the oracle) for the Poisson draw."""
-    from . import psf_gauss  # host generator, no GPU needed
+    noiseless data (the GPU projector or the oracle) for the Poisson draw.
+    ``psf_fn`` is the psf_gauss generator (default: this package's host
+    generator; a caller that must not load the CUDA library passes its own
+    restatement, bit-identical by test)."""
+    if psf_fn is None:
+        from . import psf_gauss as psf_fn  # host generator, no GPU needed
 
     rng = np.random.default_rng(seed)
     shape = (nx, nx, nz)
     image = ellipsoids(shape, k, rng, lambda i: rng.uniform(0.5, 2.0), inside_fov_bg=0.1)
     mumap = body_mumap(shape, mu_values, rng)
-    psf1 = psf_gauss(ny=nx, px=p, fwhm_start=fwhm_start, fwhm_end=fwhm_end)
+    psf1 = psf_fn(ny=nx, px=p, fwhm_start=fwhm_start, fwhm_end=fwhm_end)
     psfs = np.asfortranarray(np.repeat(psf1[:, :, :, None], nview, axis=3))
     st = Study(name, np.asfortranarray(image, np.float32), np.asfortranarray(mumap, np.float32), psfs, 4.8,
                nblocks, niter, meta=dict(seed=seed, k=k, counts=counts))
@@ -119,11 +123,11 @@ STUDIES = {
 STUDY_SEED_OFFSET = {"small_64x64x64": 0, "larger_128x128x80": 1, "large_256x256x200": 4}
 
 
-def named_study(name, project_fn=None, seed_offset=0):
+def named_study(name, project_fn=None, seed_offset=0, psf_fn=None):
     """The named study of STUDIES, generated from its fixed seed."""
     cfg = dict(STUDIES[name])
     return make_study(name, seed=BASE_SEED + STUDY_SEED_OFFSET[name] + seed_offset, project_fn=project_fn,
-                      **cfg)
+                      psf_fn=psf_fn, **cfg)
 
 
 def divisors_in(n, lo=4, hi=16):
