@@ -40,6 +40,7 @@
 #include "rot_one.cuh"
 #include "sconv.cuh"
 #include "spect_kernels.cuh"
+#include "zpath_api.h"
 
 using namespace spect;
 
@@ -224,6 +225,17 @@ struct spect_plan_s {
   // tuned launch shapes (0 = analytic default); tuned_nv = the view count they were tuned for
   int tune_fwd_cy = 0, tune_adj_cy = 0, tune_rotf_nsplit = 0, tuned_nv = 0;
   size_t rota_smem = 0;
+  // fused projector pair on z-fastest layouts (zpath.cuh): :two, attenuation
+  // cache, separable PSF planes, planes that fit in shared memory
+  int zpath = 0;
+  ZGeom zg{};
+  size_t izN = 0;              // floats of one IZ volume (L * L * nzp)
+  float* d_imgIZ = nullptr;    // forward input / OS-EM iterate (IZ)
+  float* d_backIZ = nullptr;   // back-projection accumulator (IZ)
+  float* d_Hz = nullptr;       // [nset][ny][2 hs] pass weights
+  float* d_Ez = nullptr;       // [nset][ny][2 ts] forward tails, adjoint folds
+  int zshape_fwd = -1, zshape_adj = -1;
+  size_t zfwd_smem_b = 0, zadj_smem_b = 0;
   size_t bytes = 0;
   // stream on which the plan is built and its buffers are (de)allocated;
   // async_alloc: cudaMallocAsync/cudaFreeAsync on it (no device-wide sync)
@@ -253,7 +265,7 @@ void free_plan(spect_plan_s* p) {
   void* ptrs[] = {p->d_mumap, p->d_att, p->d_err, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
-                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep};
+                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep, p->d_imgIZ, p->d_backIZ, p->d_Hz, p->d_Ez};
   for (void* q : ptrs)
     if (q) {
       if (p->async_alloc) cudaFreeAsync(q, p->home);
@@ -519,10 +531,87 @@ cudaError_t conv_launch(const spect_plan_s* p, int kind, int grid, cudaStream_t 
   return cudaErrorInvalidValue;
 }
 
+ZArgs zargs(const spect_plan_s* p) {
+  ZArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.g = p->zg;
+  a.img = p->d_imgIZ;
+  a.att = p->d_att;
+  a.H = p->d_Hz;
+  a.E = p->d_Ez;
+  a.rot = p->d_rot;
+  a.viewset = p->d_viewset;
+  a.err = p->d_err;
+  return a;
+}
+
+// zpath forward of nidx views of the IZ image: k_zfwd (rotation, attenuation,
+// convolution, depth sum of chunks) then the chunk sum (+ EM ratio y/(Ax+bg))
+int zforward(spect_plan_s* p, float* views, const float* imgIZ, const int* vidx, int nidx, cudaStream_t st,
+             const float* y, const float* bg, float* partbuf, int gmax) {
+  for (int g0 = 0; g0 < nidx; g0 += gmax) {
+    const int nv = std::min(gmax, nidx - g0);
+    const int* vi = vidx + g0;
+    int cy, nc;
+    chunking(p, nv, false, &cy, &nc);
+    ZArgs a = zargs(p);
+    a.img = imgIZ;
+    a.vidx = vi;
+    a.nv = nv;
+    a.chunkY = cy;
+    a.nchunks = nc;
+    a.part = partbuf;
+    const int gs = std::min(p->sm_count, nv * nc);
+    LAUNCH(p, K_CONV_FWD, st, "k_zfwd", zfwd_launch(p->zshape_fwd, gs, p->zfwd_smem_b, st, a));
+    const size_t n = (size_t)nv * p->nxz;
+    const int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16);
+    LAUNCH(p, K_REDUCE_VIEWS, st, "k_reduce_views",
+           k_reduce_views<<<rb, 256, 0, st>>>(partbuf, nv, nc, (int)p->nxz, views + (size_t)g0 * p->nxz, y, bg, vi));
+  }
+  return SPECT_OK;
+}
+
+// zpath adjoint of nidx views into outIZ (IZ layout): per group k_zadj (T
+// planes) then k_zrot_adj (gather over the group's views; groups after the
+// first add to the accumulator).  mode 0: out = A' views; 1: zeros -> Inf;
+// 2: out = x .* (A' views) ./ asum (x, asum in IZ; out may be x).
+int zbackward(spect_plan_s* p, float* outIZ, const float* views, const int* vidx, int nidx, cudaStream_t st, int mode,
+              const float* xIZ, const float* asumIZ) {
+  if (nidx == 0) {
+    CUDA_TRY(cudaMemsetAsync(outIZ, 0, sizeof(float) * p->izN, st));
+    return SPECT_OK;
+  }
+  const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 16, 256));
+  for (int g0 = 0; g0 < nidx; g0 += p->gmax) {
+    const int nv = std::min(p->gmax, nidx - g0);
+    const int* vi = vidx + g0;
+    int cy, nc;
+    chunking(p, nv, true, &cy, &nc);
+    ZArgs a = zargs(p);
+    a.views = views + (size_t)g0 * p->nxz;
+    a.T = p->d_P;
+    a.vidx = vi;
+    a.nv = nv;
+    a.chunkY = cy;
+    a.nchunks = nc;
+    const int gs = std::min(p->sm_count, nv * nc);
+    LAUNCH(p, K_CONV_ADJ, st, "k_zadj", zadj_launch(p->zshape_adj, gs, p->zadj_smem_b, st, a));
+    const bool last = g0 + nv >= nidx;
+    LAUNCH(p, K_ROT_ADJ, st, "k_zrot_adj",
+           zrot_adj_launch(p->zg, grot, st, p->d_P, p->d_rot, vi, nv, g0 > 0 ? p->d_backIZ : nullptr,
+                           last ? outIZ : p->d_backIZ, xIZ, asumIZ, last ? mode : 0));
+  }
+  return SPECT_OK;
+}
+
 // forward projection of nidx views (device index list vidx) into views;
 // with y/bg non-null the output is the EM ratio y/(A x + bg).
 int forward_scratch(spect_plan_s* p, float* views, const float* image, const int* vidx, int nidx, cudaStream_t st,
                     const float* y, const float* bg, float* Pbuf, float* partbuf, int gmax) {
+  if (p->zpath) {
+    LAUNCH(p, K_OTHER, st, "k_to_iz", zto_iz_launch(p->zg, st, image, p->d_imgIZ));
+    return zforward(p, views, p->d_imgIZ, vidx, nidx, st, y, bg, partbuf, gmax);
+  }
   const Geom& g = p->g;
   for (int g0 = 0; g0 < nidx; g0 += gmax) {
     const int nv = std::min(gmax, nidx - g0);
@@ -598,6 +687,11 @@ int forward(spect_plan_s* p, float* views, const float* image, const int* vidx, 
 // A' views with zeros -> Inf (EM sensitivity); mode 2: image .*= (A' views) ./ asum
 int backward(spect_plan_s* p, float* image, const float* views, const int* vidx, int nidx, cudaStream_t st,
              int mode, const float* asum) {
+  if (p->zpath) {
+    STATUS_TRY(zbackward(p, p->d_backIZ, views, vidx, nidx, st, 0, nullptr, nullptr));
+    LAUNCH(p, K_REDUCE_IMAGE, st, "k_from_iz", zfrom_iz_launch(p->zg, st, p->d_backIZ, image, asum, mode));
+    return SPECT_OK;
+  }
   const Geom& g = p->g;
   const int nsplit = p->nsplit_adj;
   if (nidx == 0) {
@@ -696,12 +790,13 @@ int ensure_em(spect_plan_s* p, int nblocks) {
   }
   if (!p->d_flag) STATUS_TRY(dalloc(p, &p->d_flag, 1));
   if (p->asum_blocks < nblocks) {
+    const size_t unit = p->zpath ? p->izN : p->N;  // one sensitivity image
     if (p->d_asum) {
       dfree(p, p->d_asum);
-      p->bytes -= sizeof(float) * p->N * p->asum_blocks;
+      p->bytes -= sizeof(float) * unit * p->asum_blocks;
     }
     p->d_asum = nullptr;
-    STATUS_TRY(dalloc(p, &p->d_asum, p->N * nblocks));
+    STATUS_TRY(dalloc(p, &p->d_asum, unit * nblocks));
     p->asum_blocks = nblocks;
   }
   return SPECT_OK;
@@ -750,6 +845,21 @@ int prepare_osem(spect_plan_s* p, int nblocks, int niter) {
 int enqueue_osem(spect_plan_s* p, float* out, const float* x0, const float* y, const float* bg, int nblocks, int niter,
                  cudaStream_t st) {
   const int nsub = p->nview / nblocks;
+  if (p->zpath) {  // the iterate and the sensitivities stay in the IZ layout
+    LAUNCH(p, K_OTHER, st, "k_to_iz", zto_iz_launch(p->zg, st, x0, p->d_imgIZ));
+    for (int b = 0; b < nblocks; ++b)
+      STATUS_TRY(zbackward(p, p->d_asum + (size_t)b * p->izN, p->d_ones, p->d_sub + (size_t)b * nsub, nsub, st, 1,
+                           nullptr, nullptr));
+    for (int it = 0; it < niter; ++it)
+      for (int b = 0; b < nblocks; ++b) {
+        const int* vi = p->d_sub + (size_t)b * nsub;
+        STATUS_TRY(zforward(p, p->d_views_tmp, p->d_imgIZ, vi, nsub, st, y, bg, p->d_part, p->gmax));
+        STATUS_TRY(zbackward(p, p->d_imgIZ, p->d_views_tmp, vi, nsub, st, 2, p->d_imgIZ,
+                             p->d_asum + (size_t)b * p->izN));
+      }
+    LAUNCH(p, K_REDUCE_IMAGE, st, "k_from_iz", zfrom_iz_launch(p->zg, st, p->d_imgIZ, out, nullptr, 0));
+    return SPECT_OK;
+  }
   for (int b = 0; b < nblocks; ++b)
     STATUS_TRY(backward(p, p->d_asum + (size_t)b * p->N, p->d_ones, p->d_sub + (size_t)b * nsub, nsub, st, 1,
                         nullptr));
@@ -810,6 +920,7 @@ int static_scratch_address(void** out) {
 struct TuneResult {
   int fwd_cy, adj_cy, rotf_nsplit, nsplit_adj, sep, sep_adj;
   double fwd_ms, adj_ms;
+  int zshape_fwd, zshape_adj;
 };
 std::mutex g_tune_mu;
 std::vector<std::pair<std::string, TuneResult>> g_tune_cache;
@@ -818,7 +929,8 @@ std::string tune_key(const spect_plan_s* p, int nv) {
   return std::to_string(p->nx) + "x" + std::to_string(p->nz) + "/" + std::to_string(p->px) + "x" +
          std::to_string(p->pz) + "/v" + std::to_string(p->nview) + "/n" + std::to_string(nv) + "/i" +
          std::to_string(p->interp) + "/a" + std::to_string(p->d_att ? 1 : 0) + "/d" + std::to_string(p->device) +
-         "/s" + std::to_string(p->sep_fwd_ok) + std::to_string(p->sep_adj_ok) + std::to_string(p->sep_forced);
+         "/s" + std::to_string(p->sep_fwd_ok) + std::to_string(p->sep_adj_ok) + std::to_string(p->sep_forced) +
+         "/z" + std::to_string(p->zpath) + "/y" + std::to_string(p->ny);
 }
 
 int time_pass(spect_plan_s* p, bool adj, int nv, int reps, double* ms) {
@@ -857,6 +969,10 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
         p->nsplit_adj = kv.second.nsplit_adj;
         p->sep = kv.second.sep && p->sep_fwd_ok;
         p->sep_adj = kv.second.sep_adj && p->sep_adj_ok;
+        if (p->zpath) {
+          p->zshape_fwd = kv.second.zshape_fwd;
+          p->zshape_adj = kv.second.zshape_adj;
+        }
         *fwd_ms = kv.second.fwd_ms;
         *adj_ms = kv.second.adj_ms;
         return SPECT_OK;
@@ -876,6 +992,55 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
   for (double c0 : {0.0, 0.25, 0.5, 1.0, 2.0, 4.0}) {
     int c = best_chunk(p, nv, c0);
     if (std::find(cys.begin(), cys.end(), c) == cys.end()) cys.push_back(c);
+  }
+  if (p->zpath) {
+    // fused path: depth tile and launch shape per direction
+    const int xtasks = p->nz * (p->nx / 8);
+    std::vector<int> fsh, ash;
+    for (int i = 0; i < kZNShapes; ++i) {
+      const int cap = kZShapes[i].nt * kZShapes[i].nth;
+      if (cap >= xtasks && cap <= 2 * xtasks) fsh.push_back(i);
+      if (kZShapes[i].nt == 1 && kZShapes[i].nth <= 640) ash.push_back(i);
+    }
+    if (fsh.empty()) fsh.push_back(p->zshape_fwd);
+    double bf = 1e300, ba = 1e300;
+    int bcy = cys[0], bacy = cys[0], bsf = p->zshape_fwd, bsa = p->zshape_adj, rc = SPECT_OK;
+    for (int sh : fsh)
+      for (int cy : cys) {
+        p->zshape_fwd = sh;
+        p->tune_fwd_cy = cy;
+        double t;
+        if ((rc = time_pass(p, false, nv, 2, &t)) != SPECT_OK) break;
+        if (t < bf) {
+          bf = t;
+          bcy = cy;
+          bsf = sh;
+        }
+      }
+    for (int sh : ash)
+      for (int cy : cys) {
+        if (rc != SPECT_OK) break;
+        p->zshape_adj = sh;
+        p->tune_adj_cy = cy;
+        double t;
+        if ((rc = time_pass(p, true, nv, 2, &t)) != SPECT_OK) break;
+        if (t < ba) {
+          ba = t;
+          bacy = cy;
+          bsa = sh;
+        }
+      }
+    p->zshape_fwd = bsf;
+    p->zshape_adj = bsa;
+    p->tune_fwd_cy = bcy;
+    p->tune_adj_cy = bacy;
+    p->prof.on = prof;
+    if (rc != SPECT_OK) return rc;
+    *fwd_ms = bf;
+    *adj_ms = ba;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache.push_back({key, TuneResult{bcy, bacy, 0, 1, p->sep, p->sep_adj, bf, ba, bsf, bsa}});
+    return SPECT_OK;
   }
   // convolution kernels to try: direct (separable planes) and FFT, unless
   // SPECT_CONV fixed the choice
@@ -936,7 +1101,7 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
   *fwd_ms = bf;
   *adj_ms = ba;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune_cache.push_back({key, TuneResult{bcy, bacy, brs, bns, bsep, basep, bf, ba}});
+  g_tune_cache.push_back({key, TuneResult{bcy, bacy, brs, bns, bsep, basep, bf, ba, -1, -1}});
   return SPECT_OK;
 }
 
@@ -1080,6 +1245,112 @@ bool psf_symmetric(const float* psfs, const std::vector<int>& stacks, size_t ny,
   return true;
 }
 
+// Factor every plane of the distinct PSF stacks as h[i, j] = a[i] b[j]
+// (rank 1 within 1e-6 of max|h|: true for psf_gauss planes), into fa
+// [set][y][px] and fb [set][y][pz] (double); Gaussian plans take the exact
+// 1-D factors.  False when some plane is not separable.
+bool factor_planes(const float* psfs, const std::vector<int>& uniq, int ny, int px, int pz, const PlanOpts& opts,
+                   std::vector<double>& fa, std::vector<double>& fb) {
+  const size_t pp = (size_t)px * pz;
+  fa.assign(uniq.size() * ny * px, 0.0);
+  fb.assign(uniq.size() * ny * pz, 0.0);
+  auto gauss_taps = [](int n, double fwhm, double* w) {
+    const int h = (n - 1) / 2;
+    if (fwhm == 0) {
+      for (int i = 0; i < n; ++i) w[i] = (i == h) ? 1.0 : 0.0;
+      return;
+    }
+    const double sigma = fwhm / std::sqrt(std::log(256.0));
+    double s = 0;
+    for (int i = 0; i < n; ++i) {
+      const double q = (double)(i - h) / sigma;
+      w[i] = std::exp(-0.5 * q * q);
+      s += w[i];
+    }
+    for (int i = 0; i < n; ++i) w[i] /= s;
+  };
+  for (size_t u = 0; u < uniq.size(); ++u)
+    for (int y = 0; y < ny; ++y) {
+      double* a = fa.data() + (u * ny + y) * px;
+      double* b = fb.data() + (u * ny + y) * pz;
+      if (opts.gauss) {
+        auto fw = [&](double f0, double f1) { return ny <= 1 ? f0 : (y == ny - 1 ? f1 : f0 + y * ((f1 - f0) / (ny - 1))); };
+        gauss_taps(px, fw(opts.gx0, opts.gx1), a);
+        gauss_taps(pz, fw(opts.gz0, opts.gz1), b);
+        continue;
+      }
+      const float* k = psfs + ((size_t)uniq[u] * ny + y) * pp;  // k[i + px j]
+      const int i0 = (px - 1) / 2, j0 = (pz - 1) / 2;
+      const double c = k[i0 + (size_t)px * j0];
+      double mx = 0;
+      for (size_t e = 0; e < pp; ++e) mx = std::max(mx, (double)std::fabs(k[e]));
+      if (!(c != 0.0) || !(mx > 0.0)) return false;
+      for (int i = 0; i < px; ++i) a[i] = k[i + (size_t)px * j0];
+      for (int j = 0; j < pz; ++j) b[j] = k[i0 + (size_t)px * j] / c;
+      double res = 0;
+      for (int j = 0; j < pz; ++j)
+        for (int i = 0; i < px; ++i) res = std::max(res, std::fabs(k[i + (size_t)px * j] - a[i] * b[j]));
+      if (res > 1e-6 * mx) return false;
+    }
+  return true;
+}
+
+// adjoint folds of a centred factor w (2h + 1 taps): cL_k = sum_{d>k} w(d),
+// cR_k = sum_{d<-k} w(d), k < h
+void fold_tails(const double* w, int h, float* L, float* R) {
+  for (int k = 0; k < h; ++k) {
+    double l = 0, r = 0;
+    for (int i = h + k + 1; i <= 2 * h; ++i) l += w[i];
+    for (int i = 0; i < h - k; ++i) r += w[i];
+    L[k] = (float)l;
+    R[k] = (float)r;
+  }
+}
+
+// forward clamp tails of the reversed factor wr[m] = w[p - 1 - m]:
+// EL[i] = sum_{m < h - i} wr[m] (i < h), ER[k] = sum_{m > h + k} wr[m] (k < h)
+void clamp_tails(const double* w, int p, float* EL, float* ER) {
+  const int h = (p - 1) / 2;
+  for (int i = 0; i < h; ++i) {
+    double l = 0, r = 0;
+    for (int m = 0; m < h - i; ++m) l += w[p - 1 - m];
+    for (int m = h + 1 + i; m < p; ++m) r += w[p - 1 - m];
+    EL[i] = (float)l;
+    ER[i] = (float)r;
+  }
+}
+
+// zpath launch shapes: forward -- the fewest thread slots holding every x
+// task of a plane (ties: more threads); adjoint -- the least padded x and z
+// passes, one task per thread and pass (no 1024-thread shape: it spills)
+int zpick_fwd(const ZGeom& g) {
+  const int xtasks = g.nz * (g.nx / 8);
+  int best = -1;
+  for (int i = 0; i < kZNShapes; ++i) {
+    const int cap = kZShapes[i].nt * kZShapes[i].nth;
+    if (cap < xtasks) continue;
+    if (best < 0 || cap < kZShapes[best].nt * kZShapes[best].nth ||
+        (cap == kZShapes[best].nt * kZShapes[best].nth && kZShapes[i].nth > kZShapes[best].nth))
+      best = i;
+  }
+  return best;
+}
+int zpick_adj(const ZGeom& g) {
+  const long long xt = (long long)g.nz * (g.nx / 8), zt = (long long)g.nx * ((g.nz + 7) / 8);
+  int best = -1;
+  long long bc = 0;
+  for (int i = 0; i < kZNShapes; ++i) {
+    const int nth = kZShapes[i].nth;
+    if (kZShapes[i].nt != 1 || nth > 640) continue;
+    const long long c = nth * ((xt + nth - 1) / nth + (zt + nth - 1) / nth);
+    if (best < 0 || c < bc) {
+      best = i;
+      bc = c;
+    }
+  }
+  return best;
+}
+
 int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, int nview, const float* mumap,
                      const float* psfs, float dy, const float* viewangle, int interpmeth, int mode, int nthread,
                      int nthreads, const PlanOpts& opts) {
@@ -1146,11 +1417,33 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     free_plan(p);
     return st;
   };
-  // attenuation cache (nview * N floats): on when it fits a quarter of the
-  // free device memory (and 32 GiB); SPECT_ATTEN_CACHE=0 turns it off
+  // separable PSF planes (host factorisation) and the fused-path decision:
+  // :two, separable planes, attenuation cache, planes that fit in shared memory
+  std::vector<double> fa, fb;
+  const bool sep_host = factor_planes(psfs, uniq, ny, px, pz, opts, fa, fb);
+  const char* conv_env = std::getenv("SPECT_CONV");
+  const bool only_fft = conv_env && std::strcmp(conv_env, "fft") == 0;
+  const int pad_rot = (int)std::ceil(1.0 + nx * std::sqrt(2.0) / 2.0 - nx / 2.0);
+  const ZGeom zg = zgeom_make(nx, ny, nz, px, pz, pad_rot);
+  bool zcand = false;
+  {
+    int dev = 0, optin = 0;
+    const char* zenv = std::getenv("SPECT_ZPATH");
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess)
+      zcand = interpmeth == SPECT_INTERP_TWO && sep_host && !only_fft && !(zenv && zenv[0] == '0') && nx % 8 == 0 &&
+              zg.nzp <= 256 && zpick_fwd(zg) >= 0 && zpick_adj(zg) >= 0 && zfwd_smem(zg) <= (size_t)optin &&
+              zadj_smem(zg) <= (size_t)optin && opts.atten_cache != 0;
+    cudaGetLastError();
+  }
+  // attenuation cache: on when it fits a quarter of the free device memory
+  // (and 32 GiB); SPECT_ATTEN_CACHE=0 turns it off (and with it the fused
+  // path).  The fused path keeps it z-fastest ([view][y][x][nzp]), the
+  // other kernels as [view][y][z][x].
   {
     const char* env = std::getenv("SPECT_ATTEN_CACHE");
-    size_t need = sizeof(float) * p->N * (size_t)nview, fr = 0, tot = 0;
+    const size_t cnt = zcand ? (size_t)nview * ny * nx * zg.nzp : p->N * (size_t)nview;
+    size_t need = sizeof(float) * cnt, fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
       cudaGetLastError();
       fr = 0;
@@ -1161,13 +1454,24 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       // the :one path reads its attenuation from the cache
       int st1 = dalloc(p, &p->d_att, p->N * (size_t)nview);
       if (st1 != SPECT_OK) return bail(st1);
-    } else if (want && dalloc(p, &p->d_att, p->N * (size_t)nview) != SPECT_OK) {
+    } else if (want && dalloc(p, &p->d_att, cnt) != SPECT_OK) {
       p->d_att = nullptr;
       g_err.clear();
     }
+    p->zpath = (zcand && p->d_att) ? 1 : 0;
   }
   int st = configure(p);
   if (st != SPECT_OK) return bail(st);
+  if (p->zpath) {
+    p->zg = zg;
+    p->izN = (size_t)zg.L * zg.L * zg.nzp;
+    p->zshape_fwd = zpick_fwd(zg);
+    p->zshape_adj = zpick_adj(zg);
+    p->zfwd_smem_b = zfwd_smem(zg);
+    p->zadj_smem_b = zadj_smem(zg);
+    const cudaError_t ze = zpath_setup((int)p->max_smem);
+    if (ze != cudaSuccess) return bail(fail(SPECT_ERR_CUDA, std::string("fused kernel setup: ") + cudaGetErrorString(ze)));
+  }
 
   // angles: default (0:nview-1)/nview * Float32(2pi), element rounded to Float32
   p->angles.resize(nview);
@@ -1183,8 +1487,11 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
   p->nset = (int)uniq.size();
 
   // group size: rotated-plane scratch bounded by ~1 GiB
+  // (the fused path's adjoint planes T hold nzp >= nz values per column)
   const size_t budget = (size_t)1 << 30;
-  p->gmax = (int)std::max<size_t>(1, std::min<size_t>((size_t)nview, budget / (sizeof(float) * p->N)));
+  const size_t slot = p->zpath ? (size_t)ny * nx * zg.nzp : p->N;
+  if (p->zpath) p->nsplit_adj = p->nsplit_adj_max = 1;  // no split partial images
+  p->gmax = (int)std::max<size_t>(1, std::min<size_t>((size_t)nview, budget / (sizeof(float) * slot)));
   if (opts.gmax_cap > 0) p->gmax = std::min(p->gmax, opts.gmax_cap);
 
   if ((st = dalloc(p, &p->d_mumap, p->N)) || (st = dalloc(p, &p->d_rot, nview)) ||
@@ -1193,12 +1500,20 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       (st = (cudaMemsetAsync(p->d_err, 0, sizeof(int), p->home) == cudaSuccess) ? SPECT_OK
                                                                                  : fail(SPECT_ERR_CUDA, "memset")) ||
       (st = dalloc(p, &p->d_H, (size_t)p->nset * ny * (p->cg.Q + 1) * Npx)) ||
-      (st = dalloc(p, &p->d_P, (size_t)p->gmax * p->N)) ||
+      (st = dalloc(p, &p->d_P, (size_t)p->gmax * slot)) ||
       (st = ((p->nchunk_max = ((size_t)p->gmax * 32 * p->nxz * 4 <= ((size_t)256 << 20)) ? 32 : 16),
              dalloc(p, &p->d_part, (size_t)p->gmax * p->nchunk_max * p->nxz))) ||
       (st = dalloc(p, &p->d_Vs, (size_t)p->gmax * p->cg.Q * Npx)) ||
       (st = dalloc(p, &p->d_imgpart, (size_t)p->nsplit_adj_max * p->N)))
     return bail(st);
+  if (p->zpath) {  // IZ volumes (zero ring and z padding) and zeroed adjoint planes
+    if ((st = dalloc(p, &p->d_imgIZ, p->izN)) || (st = dalloc(p, &p->d_backIZ, p->izN)))
+      return bail(st);
+    cudaError_t e = cudaMemsetAsync(p->d_imgIZ, 0, sizeof(float) * p->izN, p->home);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->d_backIZ, 0, sizeof(float) * p->izN, p->home);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->d_P, 0, sizeof(float) * (size_t)p->gmax * slot, p->home);
+    if (e != cudaSuccess) return bail(fail(SPECT_ERR_CUDA, std::string("memset: ") + cudaGetErrorString(e)));
+  }
 
   std::vector<float2> tw(SPECT_TW_N);
   for (int m = 0; m < SPECT_TW_N; ++m) {
@@ -1280,6 +1595,20 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       fail(SPECT_ERR_CUDA, std::string("attenuation cache (:one): ") + cudaGetErrorString(e));
       return bail(SPECT_ERR_CUDA);
     }
+  } else if (p->d_att && p->zpath) {
+    // z-fastest cache from the mu-map laid out on the padded grid
+    float* muz = nullptr;
+    cudaError_t e = p->async_alloc ? cudaMallocAsync((void**)&muz, sizeof(float) * p->izN, hs)
+                                   : cudaMalloc((void**)&muz, sizeof(float) * p->izN);
+    if (e == cudaSuccess) e = cudaMemsetAsync(muz, 0, sizeof(float) * p->izN, hs);
+    if (e == cudaSuccess) e = zto_iz_launch(p->zg, hs, p->d_mumap, muz);
+    if (e == cudaSuccess) e = zatten_launch(p->zg, nview, hs, muz, p->d_rot, dy, p->d_att);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(hs);
+    if (muz) dfree(p, muz);
+    if (e != cudaSuccess) {
+      fail(SPECT_ERR_CUDA, std::string("attenuation cache: ") + cudaGetErrorString(e));
+      return bail(SPECT_ERR_CUDA);
+    }
   } else if (p->d_att) {
     dim3 grid(nz, std::max(1, std::min(cdiv(2 * p->sm_count, nz), cdiv(nview, p->rotf_vpb))));
     const int thr = nx * p->rotf_vpb;
@@ -1357,56 +1686,21 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       return bail(SPECT_ERR_CUDA);
     }
   }
-  // separable PSF planes: factor every distinct stack's planes h = a b^T
+  // separable PSF planes: weight tables from the factors h = a b^T
   {
     const int zp = sep_zp(pz), xp = sep_xp(px), hs = zp + xp, hxs = (px - 1) / 2, hzs = (pz - 1) / 2;
     const int ts = std::max(4, (2 * hxs + 2 * hzs + 3) & ~3);
     std::vector<float> H((size_t)p->nset * ny * 2 * hs, 0.f), Tl((size_t)p->nset * ny * ts, 0.f);
-    bool ok = true;
-    std::vector<double> a(px), b(pz);
-    auto gauss_taps = [](int n, double fwhm, std::vector<double>& w) {
-      const int h = (n - 1) / 2;
-      if (fwhm == 0) {
-        for (int i = 0; i < n; ++i) w[i] = (i == h) ? 1.0 : 0.0;
-        return;
-      }
-      const double sigma = fwhm / std::sqrt(std::log(256.0));
-      double s = 0;
-      for (int i = 0; i < n; ++i) {
-        const double q = (double)(i - h) / sigma;
-        w[i] = std::exp(-0.5 * q * q);
-        s += w[i];
-      }
-      for (auto& v : w) v /= s;
-    };
-    for (int u = 0; u < p->nset && ok; ++u)
-      for (int y = 0; y < ny && ok; ++y) {
-        if (opts.gauss) {
-          auto fw = [&](double f0, double f1) {
-            return ny <= 1 ? f0 : (y == ny - 1 ? f1 : f0 + y * ((f1 - f0) / (ny - 1)));
-          };
-          gauss_taps(px, fw(opts.gx0, opts.gx1), a);
-          gauss_taps(pz, fw(opts.gz0, opts.gz1), b);
-        } else {
-          const float* k = psfs + ((size_t)uniq[u] * ny + y) * pp;  // k[i + px j]
-          const int i0 = (px - 1) / 2, j0 = (pz - 1) / 2;
-          const double c = k[i0 + (size_t)px * j0];
-          double mx = 0;
-          for (size_t e = 0; e < pp; ++e) mx = std::max(mx, (double)std::fabs(k[e]));
-          if (!(c != 0.0) || !(mx > 0.0)) {
-            ok = false;
-            break;
-          }
-          for (int i = 0; i < px; ++i) a[i] = k[i + (size_t)px * j0];
-          for (int j = 0; j < pz; ++j) b[j] = k[i0 + (size_t)px * j] / c;
-          double res = 0;
-          for (int j = 0; j < pz; ++j)
-            for (int i = 0; i < px; ++i) res = std::max(res, std::fabs(k[i + (size_t)px * j] - a[i] * b[j]));
-          if (res > 1e-6 * mx) {
-            ok = false;
-            break;
-          }
-        }
+    const bool ok = sep_host;
+    std::vector<float> Hz, Ez;
+    if (ok && p->zpath) {
+      Hz.assign((size_t)p->nset * ny * 2 * zg.hs, 0.f);
+      Ez.assign((size_t)p->nset * ny * 2 * zg.ts, 0.f);
+    }
+    for (int u = 0; ok && u < p->nset; ++u)
+      for (int y = 0; y < ny; ++y) {
+        const double* a = fa.data() + ((size_t)u * ny + y) * px;
+        const double* b = fb.data() + ((size_t)u * ny + y) * pz;
         // [wz reversed | wx reversed | b | a], each zero-padded (zp, xp)
         float* hrow = H.data() + ((size_t)u * ny + y) * 2 * hs;
         for (int m = 0; m < pz; ++m) hrow[m] = (float)b[pz - 1 - m];
@@ -1415,18 +1709,29 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
         for (int m = 0; m < px; ++m) hrow[hs + zp + m] = (float)a[m];
         // adjoint edge tails: cL_k = sum_{d>k} w(d), cR_k = sum_{d<-k} w(d)
         float* trow = Tl.data() + ((size_t)u * ny + y) * ts;
-        auto tails = [](const std::vector<double>& w, int h, float* L, float* R) {
-          for (int k = 0; k < h; ++k) {
-            double l = 0, r = 0;
-            for (int i = h + k + 1; i <= 2 * h; ++i) l += w[i];
-            for (int i = 0; i < h - k; ++i) r += w[i];
-            L[k] = (float)l;
-            R[k] = (float)r;
-          }
-        };
-        tails(a, hxs, trow, trow + hxs);
-        tails(b, hzs, trow + 2 * hxs, trow + 2 * hxs + hzs);
+        fold_tails(a, hxs, trow, trow + hxs);
+        fold_tails(b, hzs, trow + 2 * hxs, trow + 2 * hxs + hzs);
+        if (!Hz.empty()) {
+          // fused path: [fwd z | fwd x | adj z | adj x], each shifted right by
+          // its data offset minus the half width; tails [ELz ERz ELx ERx |
+          // cLx cRx cLz cRz]
+          const int sz = zg.R0 - zg.hz, sx = zg.C0 - zg.hx;
+          float* zr = Hz.data() + ((size_t)u * ny + y) * 2 * zg.hs;
+          for (int m = 0; m < pz; ++m) zr[sz + m] = (float)b[pz - 1 - m];
+          for (int m = 0; m < px; ++m) zr[zg.zpw + sx + m] = (float)a[px - 1 - m];
+          for (int m = 0; m < pz; ++m) zr[zg.hs + sz + m] = (float)b[m];
+          for (int m = 0; m < px; ++m) zr[zg.hs + zg.zpw + sx + m] = (float)a[m];
+          float* er = Ez.data() + ((size_t)u * ny + y) * 2 * zg.ts;
+          clamp_tails(b, pz, er, er + hzs);
+          clamp_tails(a, px, er + 2 * hzs, er + 2 * hzs + hxs);
+          std::memcpy(er + zg.ts, trow, sizeof(float) * (2 * hxs + 2 * hzs));
+        }
       }
+    if (!Hz.empty()) {
+      if ((st = dalloc(p, &p->d_Hz, Hz.size())) || (st = up(p->d_Hz, Hz.data(), sizeof(float) * Hz.size())) ||
+          (st = dalloc(p, &p->d_Ez, Ez.size())) || (st = up(p->d_Ez, Ez.data(), sizeof(float) * Ez.size())))
+        return bail(st);
+    }
     if (ok) {
       if ((st = dalloc(p, &p->d_Hsep, H.size())) || (st = up(p->d_Hsep, H.data(), sizeof(float) * H.size())) ||
           (st = dalloc(p, &p->d_Tsep, Tl.size())) || (st = up(p->d_Tsep, Tl.data(), sizeof(float) * Tl.size())))
@@ -1438,9 +1743,7 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       p->sep_fwd_smem = sconv_fwd_smem(nx, nz, px, pz, att);
       // SPECT_CONV=fft: FFT kernels only; SPECT_CONV=direct: direct kernels
       // wherever they run (neither is then re-chosen by the autotuner)
-      const char* cm = std::getenv("SPECT_CONV");
-      const bool only_fft = cm && std::strcmp(cm, "fft") == 0;
-      p->sep_forced = only_fft ? 1 : (cm && std::strcmp(cm, "direct") == 0) ? 2 : 0;
+      p->sep_forced = only_fft ? 1 : (conv_env && std::strcmp(conv_env, "direct") == 0) ? 2 : 0;
       p->sep_shape_fwd = nx % kSepXB == 0 ? sep_pick_shape(nx, nz, px, pz, true) : -1;
       p->sep_shape_adj = nx % kSepXB == 0 ? sep_pick_shape(nx, nz, px, pz, false) : -1;
       p->sep_fwd_ok = (p->sep_shape_fwd >= 0 && p->sep_fwd_smem <= p->max_smem) ? 1 : 0;
@@ -1458,6 +1761,7 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
                                       (int)p->max_smem));
     }
   }
+  if (p->zpath) p->sep_fwd_ok = p->sep_adj_ok = p->sep = p->sep_adj = 1;  // direct convolution, fused
   *out = p;
   return SPECT_OK;
 }
@@ -1524,7 +1828,9 @@ int spect_project_static_scratch(spect_plan_t p, float* views, const float* imag
                     " bytes of scratch, above the static limit of " + std::to_string(kStaticScratchBytes) + " bytes");
   void* base = nullptr;
   STATUS_TRY(static_scratch_address(&base));
-  const int gmax = (int)std::min<size_t>(G, (size_t)p->nview);
+  // groups never exceed the plan's own group size (the :one path stages
+  // rotated slices in the plan buffer sized for p->gmax views)
+  const int gmax = (int)std::min<size_t>(std::min<size_t>(G, (size_t)p->nview), (size_t)p->gmax);
   float* Pbuf = static_cast<float*>(base);
   size_t off = (sizeof(float) * (size_t)gmax * p->N + 255) & ~(size_t)255;
   float* partbuf = reinterpret_cast<float*>(static_cast<unsigned char*>(base) + off);

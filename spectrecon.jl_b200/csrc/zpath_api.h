@@ -1,0 +1,106 @@
+// zpath_api.h -- host-visible part of the fused projector pair (zpath.cuh):
+// geometry of the z-fastest layouts, kernel arguments, shared-memory sizes and
+// the launchers defined in zpath_inst.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace spect {
+
+// sizes shared by the zpath kernels (computed once per plan on the host)
+struct ZGeom {
+  int nx, ny, nz, nzp, L, pad;
+  float c0;         // rotation centre (nx - 1)/2, 0-based
+  int px, pz, hx, hz;
+  int R0, C0;       // first data row (z pass) / column (x pass) of the padded buffers
+  int zpw, xpw;     // window taps of the z and x passes (shifted, multiples of 8)
+  int hs, ts;       // weight-row and tail-row lengths of one direction
+  int rows, ast;    // z-pass buffer: rows per column, column stride (4 * odd)
+  int bs;           // x-pass buffer row stride (4 * odd)
+};
+
+__host__ __device__ constexpr int zround(int v, int m) { return (v + m - 1) / m * m; }
+// smallest 4 * odd >= v: 16-byte rows whose float4 chunk index is odd, so the
+// eight lanes of a 128-bit shared access phase hit distinct bank groups
+__host__ __device__ constexpr int zstride4(int v) {
+  return ((zround(v, 4) / 4) % 2 == 1) ? zround(v, 4) : zround(v, 4) + 4;
+}
+
+inline ZGeom zgeom_make(int nx, int ny, int nz, int px, int pz, int pad) {
+  ZGeom g{};
+  g.nx = nx;
+  g.ny = ny;
+  g.nz = nz;
+  g.nzp = zround(nz, 16);
+  g.pad = pad;
+  g.L = nx + 2 * pad;
+  g.c0 = (float)((nx - 1) * 0.5);
+  g.px = px;
+  g.pz = pz;
+  g.hx = (px - 1) / 2;
+  g.hz = (pz - 1) / 2;
+  g.R0 = zround(g.hz, 4);
+  g.C0 = zround(g.hx, 4);
+  g.zpw = zround(g.R0 - g.hz + pz, 8);
+  g.xpw = zround(g.C0 - g.hx + px, 8);
+  g.hs = g.zpw + g.xpw;
+  g.ts = zround(2 * g.hx + 2 * g.hz, 4) < 4 ? 4 : zround(2 * g.hx + 2 * g.hz, 4);
+  g.rows = zround(nz, 8) + g.zpw;
+  g.ast = zstride4(g.rows);
+  g.bs = zstride4(nx + g.xpw);
+  return g;
+}
+
+struct ZArgs {
+  ZGeom g;
+  const float* img;     // IZ
+  const float* att;     // ATT
+  const float* H;       // [set][y][2 hs]: fwd z | fwd x | adj z | adj x
+  const float* E;       // [set][y][2 ts]: ELz ERz ELx ERx | cLx cRx cLz cRz
+  const float4* rot;    // [view] (cos(2pi - theta), sin(2pi - theta), theta == 0, theta)
+  const int* vidx;      // [nv] plan view of each slot
+  const int* viewset;   // [nview] PSF set of each view
+  int nv, chunkY, nchunks;
+  float* part;          // k_zfwd output [nv][nchunks][nz][nx]
+  const float* views;   // k_zadj input [nv][nz][nx]
+  float* T;             // k_zadj output [nv][ny][nx][nzp]
+  int* err;
+};
+
+// k_zfwd shared memory (floats; every region 16-byte aligned):
+//   [bar 4][stage: att plane nx*nzp | weights hs | tails ts][Hw 2 x (hs + ts)]
+//   [PA nx, PB ny (float2)][geoW nx (float4)][geoO nx (int), rounded to 4]
+//   [ZB nx * ast][XB nz * bs]
+__host__ __device__ inline size_t zfwd_smem(const ZGeom& g) {
+  const size_t f = 4 + (size_t)g.nx * g.nzp + g.hs + g.ts + 2 * (size_t)(g.hs + g.ts) + 2 * (size_t)(g.nx + g.ny) +
+                   4 * (size_t)g.nx + zround(g.nx, 4) + (size_t)g.nx * g.ast + (size_t)g.nz * g.bs;
+  return f * sizeof(float);
+}
+
+// k_zadj shared memory (floats): [bar 4][2 stages x (hs + ts)]
+//   [VB nz * bs: the view, zero-padded, data columns C0..][WB nx * ast:
+//   x-pass output, column x, data rows R0..]
+__host__ __device__ inline size_t zadj_smem(const ZGeom& g) {
+  return sizeof(float) * (4 + 2 * (size_t)(g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)g.nx * g.ast);
+}
+
+// launch shapes of k_zfwd / k_zadj: NT tasks per thread, NTH threads
+struct ZShape {
+  int nt, nth;
+};
+constexpr int kZNShapes = 8;
+constexpr ZShape kZShapes[kZNShapes] = {{1, 512}, {2, 512}, {3, 512}, {4, 512}, {1, 640}, {2, 640}, {3, 640}, {1, 1024}};
+
+// launchers (zpath_inst.cu)
+cudaError_t zpath_setup(int max_smem);
+cudaError_t zfwd_launch(int shape, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
+cudaError_t zadj_launch(int shape, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
+cudaError_t zrot_adj_launch(const ZGeom& g, int grid, cudaStream_t st, const float* T, const float4* rot,
+                            const int* vidx, int nv, const float* prev, float* out, const float* x, const float* asum,
+                            int mode);
+cudaError_t zto_iz_launch(const ZGeom& g, cudaStream_t st, const float* img, float* iz);
+cudaError_t zfrom_iz_launch(const ZGeom& g, cudaStream_t st, const float* iz, float* dst, const float* asum, int mode);
+cudaError_t zatten_launch(const ZGeom& g, int nview, cudaStream_t st, const float* muz, const float4* rot, float dy,
+                          float* att);
+
+}  // namespace spect
