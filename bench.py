@@ -147,6 +147,91 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def peaks(S, L):
+    """Roofline denominators: the FP32 pipe measured here by the library's FFMA
+    chain probe (spect_fp32_peak), and the HBM copy bandwidth of
+    MEASURED_PEAKS.json when present (else the earlier pool measurement)."""
+    fp = ctypes.c_double(0.0)
+    S.check(L.spect_fp32_peak(ctypes.byref(fp)))
+    hbm, src = 6650.0, "fallback (6.65 TB/s, earlier measurement on this pool)"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        if m.get("hbm_gbs"):
+            hbm, src = float(m["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, ValueError):
+        pass
+    return {"fp32_tflops": round(fp.value, 2), "fp32_source": "measured FFMA chains (spect_fp32_peak), this run",
+            "hbm_gbs": hbm, "hbm_source": src}
+
+
+def launch_work(plan, kind, nv):
+    """(kernel name, bound, algorithmic FLOPs, algorithmic bytes) of one launch
+    of kernel kind `kind` processing nv views, for the path the plan runs.
+    FLOPs count the convolution taps (1 FMA = 2 FLOP per tap of the z and x
+    passes) plus the bilinear sample and attenuation; bytes count each
+    compulsory array once (attenuation planes, adjoint planes, images)."""
+    nx, ny, nz = plan.imgsize
+    px, pz = plan.px, plan.pz
+    N, nxz = nx * ny * nz, nx * nz
+    nzp = 16 * ((nz + 15) // 16)
+    if plan.fused:
+        table = {
+            "k_conv_fwd": ("k_zfwd", "fp32", nv * ny * nx * nz * (2.0 * (px + pz) + 8), 4.0 * (nv * ny * nx * nzp + N)),
+            "k_conv_adj": ("k_zadj", "fp32", nv * ny * nx * nz * (2.0 * (px + pz) + 1), 4.0 * (2 * nv * ny * nx * nzp + nv * nxz)),
+            "k_rot_adj": ("k_zrot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * ny * nx * nzp + 3 * N)),
+            "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz),
+            "k_reduce_image": ("k_from_iz", "hbm", 0.0, 4.0 * 2 * N),
+        }
+    else:
+        conv = plan.conv_kernels()
+        Npx = 1 << int(np.ceil(np.log2(nx + px - 1)))
+        Npz = 1 << int(np.ceil(np.log2(nz + pz - 1)))
+        cf = {"direct": direct_flops(nv, ny, nx, nz, px, pz), "fft": fft_flops(nv, ny, Npx, Npz)}
+        table = {
+            "k_rot_fwd": ("k_rot_fwd", "hbm", 8.0 * nv * N, 4.0 * (N + nv * N)),
+            "k_conv_fwd": ("k_sconv_fwd" if conv["forward"] == "direct" else "k_conv_fwd2", "fp32",
+                           cf[conv["forward"]], 4.0 * (2 * nv * N)),
+            "k_conv_adj": ("k_sconv_adj" if conv["adjoint"] == "direct" else "k_conv_adj2", "fp32",
+                           cf[conv["adjoint"]], 4.0 * (2 * nv * N)),
+            "k_rot_adj": ("k_rot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * N + N)),
+            "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz),
+            "k_reduce_image": ("k_reduce_image", "hbm", 0.0, 4.0 * 3 * N),
+        }
+    return table.get(kind)
+
+
+def kernel_table(plan, kms, kn, steps, nv, pk, min_share=0.10):
+    """Per-kernel time split and, for every kernel with at least `min_share`
+    of the step, its roofline against its own bound: achieved = algorithmic
+    work per launch / average CUDA-event launch time."""
+    total = sum(kms.values()) or 1.0
+    rows = []
+    for k, ms in kms.items():
+        if kn[k] == 0 or ms <= 0:
+            continue
+        w = launch_work(plan, k, nv)
+        avg = ms / kn[k]
+        row = {"kernel": w[0] if w else k, "ms_per_step": round(ms / steps, 3),
+               "launches_per_step": int(kn[k] // steps), "share": round(ms / total, 3),
+               "avg_launch_ms": round(avg, 4)}
+        if w:
+            name, bound, flops, nbytes = w
+            tf = flops / (avg / 1e3) / 1e12
+            gbs = nbytes / (avg / 1e3) / 1e9
+            if bound == "fp32":
+                row.update(bound="fp32", achieved=round(tf, 3), peak=pk["fp32_tflops"], unit="TFLOP/s",
+                           frac=round(tf / pk["fp32_tflops"], 4))
+            else:
+                row.update(bound="hbm", achieved=round(gbs, 1), peak=pk["hbm_gbs"], unit="GB/s",
+                           frac=round(gbs / pk["hbm_gbs"], 4))
+            row.update(flops_per_launch=flops, algorithmic_bytes_per_launch=nbytes,
+                       algorithmic_gbs=round(gbs, 1))
+        rows.append(row)
+    rows.sort(key=lambda r: -r["share"])
+    return rows, [r for r in rows if r["share"] >= min_share and "bound" in r]
+
+
 def build_study(S, plan_factory):
     from importlib import import_module
 
@@ -258,39 +343,24 @@ def run_ours(args):
     e2e_ms, e2e_value = agg["ms"], agg["value"]
     rel = float(np.abs(out_p.numpy().T - out_d.cpu().numpy().T).max() / np.abs(out_d.cpu().numpy()).max())
 
-    # roofline of the dominant kernel (FP32 pipe; the convolution, by FFT or
-    # by the direct separable kernels, whichever the autotuner kept)
+    # per-kernel split and rooflines (every kernel with >= 10 % of the step)
     kms = {k: ms_k[i] for i, k in enumerate(KERNELS)}
     kn = {k: n_k[i] for i, k in enumerate(KERNELS)}
-    dom = max(("k_conv_fwd", "k_conv_adj"), key=lambda k: kms[k])
     conv = plan.conv_kernels()
-    direct = conv["forward" if dom == "k_conv_fwd" else "adjoint"] == "direct"
-    Npx = 1 << int(np.ceil(np.log2(nx + plan.px - 1)))
-    Npz = 1 << int(np.ceil(np.log2(nz + plan.pz - 1)))
     nsub = nview // nb
-    if direct:
-        flops_launch = direct_flops(nsub, ny, nx, nz, plan.px, plan.pz)
-        kname = dom.replace("k_conv", "k_sconv")
-    else:
-        flops_launch = fft_flops(nsub, ny, Npx, Npz)
-        kname = dom
-    avg_ms = kms[dom] / max(kn[dom], 1)
-    achieved = flops_launch / (avg_ms / 1e3) / 1e12
-    peak = measure_fp32_peak(torch)
-    traffic = read_traffic(f"{kname}_c2.md")
-    roofline = {"bound": "fp32", "achieved": round(achieved, 3), "peak": round(peak, 2), "unit": "TFLOP/s",
-                "frac": round(achieved / peak, 4), "traffic": traffic, "kernel": kname,
-                "convolution": conv["forward" if dom == "k_conv_fwd" else "adjoint"],
-                "peak_source": "measured cuBLAS SGEMM (TF32 off) in this run",
-                "flops_per_launch": flops_launch, "avg_launch_ms": round(avg_ms, 4),
-                # DRAM bytes of one launch (ncu capture in profiles/) over its live duration
-                "hbm_gbs": round(traffic / (avg_ms / 1e3) / 1e9, 1) if traffic and avg_ms > 0 else None,
-                "kernel_ms_per_step": {k: round(v / args.steps, 3) for k, v in kms.items()},
-                "kernel_launches_per_step": {k: int(v // args.steps) for k, v in kn.items()}}
+    pk = peaks(S, L)
+    split, roofs = kernel_table(plan, kms, kn, args.steps, nsub, pk)
+    dom = dict(roofs[0]) if roofs else {}
+    traffic = read_traffic(f"{dom.get('kernel')}_c2.md") if dom else None
+    roofline = dict(dom, traffic=traffic, traffic_source="ncu dram bytes per launch (profiles/)" if traffic else None,
+                    peak_source=pk["fp32_source"] if dom.get("bound") == "fp32" else pk["hbm_source"])
     batched = served = None
     if not args.no_extras:
         batched = run_batched(S, torch)
         served = run_served(S, njobs=args.served_jobs, rate=args.served_rate)
+    studies = None
+    if not args.no_extras and ws == 1:
+        studies = {n: run_study(S, L, torch, n, args, pk, flush) for n in ("small_64x64x64", "large_256x256x200")}
     cpu = parity = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         gpu_out = np.asfortranarray(out_d.cpu().numpy().T)
@@ -299,14 +369,16 @@ def run_ours(args):
         "metric": METRIC, "value": round(value, 3), "unit": "recons/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantoms)",
-        "config": dict(CONFIG), "path": "fused OS-EM (device-resident), autotuned launch shapes",
+        "config": dict(CONFIG),
+        "path": ("fused projector pair" if plan.fused else "split kernels") + " (device-resident OS-EM), autotuned",
         "convolution": {"forward": conv["forward"], "adjoint": conv["adjoint"]}, "parity": parity,
         "e2e": {"value": round(e2e_value, 3), "unit": "recons/s",
                 "h2d_bytes_per_step": int(4 * (plan.imgsize[0] * ny * nz + 2 * nx * nz * nview)),
                 "d2h_bytes_per_step": int(4 * nx * ny * nz), "ms_per_step": round(e2e_ms / e2e_steps, 3),
                 "max_rel_diff_vs_device_path": rel},
-        "gpu_launches": int(launches), "roofline": roofline, "clocks": clk.summary(),
-        "cpu_baseline": cpu, "batched": batched, "served": served,
+        "gpu_launches": int(launches), "roofline": roofline, "kernels": roofs, "kernel_split": split,
+        "peaks": pk, "clocks": clk.summary(), "cpu_baseline": cpu, "batched": batched, "served": served,
+        "studies": studies,
     }
     if rank == 0:
         print(json.dumps(res), flush=True)
@@ -381,6 +453,26 @@ def run_batched(S, torch, njobs=32, timed_runs=2, plain_sample=6, seed=3):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / timed_runs
     launches = (L.spect_kernel_launches() - l0) // timed_runs
+    # the same jobs one after another through the device-resident spect_osem
+    # (one call per job on one stream): what the graph adds over sequential
+    # device-resident calls
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    seq_outs = [torch.zeros_like(o) for o in outs]
+
+    def seq_all():
+        for k, st in enumerate(studies):
+            x0, y, b = keep[k]
+            S.check(L.spect_osem(plans[k].handle, seq_outs[k].data_ptr(), x0.data_ptr(), y.data_ptr(), b.data_ptr(),
+                                 jobs[k]["nblocks"], jobs[k]["niter"], sp))
+
+    seq_all()
+    torch.cuda.synchronize()
+    e0.record()
+    seq_all()
+    e1.record()
+    torch.cuda.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    seq_rel = max(float((a - b).abs().max() / b.abs().max()) for a, b in zip(outs, seq_outs))
     # plain per-call path on a sample of the jobs (wall clock: it is host driven)
     t_plain = []
     rel = 0.0
@@ -400,7 +492,10 @@ def run_batched(S, torch, njobs=32, timed_runs=2, plain_sample=6, seed=3):
     return {"jobs": njobs, "recons_per_s": round(batched, 3), "ms_per_batch": round(ms, 2),
             "plain_percall_recons_per_s": round(plain, 3), "plain_sample_jobs": len(t_plain),
             "speedup_vs_plain": round(batched / plain, 2), "graph_kernels": int(launches),
-            "max_rel_diff_vs_plain": rel}
+            "max_rel_diff_vs_plain": rel,
+            "sequential_device_recons_per_s": round(njobs / (seq_ms / 1e3), 3),
+            "speedup_vs_sequential_device": round(batched / (njobs / (seq_ms / 1e3)), 2),
+            "max_rel_diff_vs_sequential_device": seq_rel}
 
 
 def run_served(S, njobs=500, rate=10.0, big_fraction=0.1, seed=4, pool_small=36, pool_big=3, plain_sample=10,
@@ -453,7 +548,9 @@ def run_served(S, njobs=500, rate=10.0, big_fraction=0.1, seed=4, pool_small=36,
         return lat, wall, stats
 
     lat, wall, stats = stream(njobs, rate)
-    slat, swall, sstats = stream(saturated_jobs, None)
+    sat = [stream(saturated_jobs, None) for _ in range(3)]  # saturated, three times
+    sat.sort(key=lambda r: r[1])
+    slat, swall, sstats = sat[1]  # the median run
     # plain per-call path on a sample with the same share of big jobs
     nbig = max(1, int(round(plain_sample * big_fraction)))
     sample = [k for k in picks if k < nsm][: plain_sample - nbig] + [k for k in picks if k >= nsm][:nbig]
@@ -478,32 +575,128 @@ def run_served(S, njobs=500, rate=10.0, big_fraction=0.1, seed=4, pool_small=36,
             "saturated": {"requests": saturated_jobs, "recons_per_s": round(saturated_jobs / swall, 3),
                           "p50_ms": round(float(np.percentile(slat, 50)), 1),
                           "p99_ms": round(float(np.percentile(slat, 99)), 1),
-                          "max_active": int(sstats["max_active_seen"])},
+                          "max_active": int(sstats["max_active_seen"]),
+                          "runs": 3, "recons_per_s_min_med_max": [round(saturated_jobs / r[1], 3) for r in
+                                                                  (sat[2], sat[1], sat[0])]},
             "plain_percall_recons_per_s": round(plain, 3), "plain_sample_jobs": len(sample),
             "plain_includes_plan_creation": True,
             "speedup_vs_plain": round(served / plain, 2),
             "saturated_speedup_vs_plain": round(saturated_jobs / swall / plain, 2)}
 
 
-def measure_fp32_peak(torch):
-    """FP32 (non-tensor) peak: cuBLAS SGEMM 8192^3 with TF32 disabled, best of 5."""
-    prev = torch.backends.cuda.matmul.allow_tf32
-    torch.backends.cuda.matmul.allow_tf32 = False
-    n = 8192
-    a = torch.randn(n, n, device="cuda")
-    b = torch.randn(n, n, device="cuda")
-    c = a @ b
-    best = 0.0
-    for _ in range(5):
+def run_study(S, L, torch, name, args, pk, flush):
+    """One named study beside the benchmark line: device-resident
+    reconstructions/s (CUDA events, L2 flushed), end to end through the host
+    C-ABI call, the per-kernel split and rooflines, and the error of the GPU
+    result against the Float32 and Float64 oracle -- the full reconstruction
+    for the 64^3 ML-EM study (whose oracle run is also its CPU time), one
+    OS-EM subset update (sensitivity of subset 0, then its update from a
+    uniform start) for the 256x256x200 study, whose full oracle
+    reconstruction would take tens of minutes."""
+    from importlib import import_module
+
+    from oracle import oracle as O
+
+    W = import_module("spectrecon_b200.workloads")
+
+    def proj(image, s):
+        plan = S.SPECTplan(s.mumap, s.psfs, s.dy)
+        v = S.project(image, plan)
+        plan.close()
+        return v
+
+    st = W.named_study(name, project_fn=proj)
+    plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    nx, ny, nz = plan.imgsize
+    nb, niter = st.nblocks, st.niter
+    nsub = st.nview // nb
+    plan.autotune(nsub)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a, np.float32).T)).cuda()
+    x0_h = np.ones((nx, ny, nz), np.float32, order="F")
+    x0_d, y_d, b_d = dev(x0_h), dev(st.ynoisy), dev(st.background)
+    out_d = torch.empty_like(x0_d)
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        S.check(L.spect_osem(plan.handle, out_d.data_ptr(), x0_d.data_ptr(), y_d.data_ptr(), b_d.data_ptr(),
+                             nb, niter, sp))
+
+    for _ in range(max(3, args.warmup)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    S.check(L.spect_plan_profile(plan.handle, 1))
+    steps = max(3, min(args.steps, 10))
+    times = []
+    for _ in range(steps):
+        flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.matmul(a, b, out=c)
-        e1.record()
+        e0.record(stream)
+        step()
+        e1.record(stream)
         torch.cuda.synchronize()
-        best = max(best, 2 * n ** 3 / (e0.elapsed_time(e1) / 1e3) / 1e12)
-    torch.backends.cuda.matmul.allow_tf32 = prev
-    del a, b, c
-    return best
+        times.append(e0.elapsed_time(e1))
+    ms_k = (ctypes.c_double * 8)()
+    n_k = (ctypes.c_longlong * 8)()
+    S.check(L.spect_plan_kernel_times(plan.handle, ms_k, n_k))
+    S.check(L.spect_plan_profile(plan.handle, 0))
+    kms = {k: ms_k[i] for i, k in enumerate(KERNELS)}
+    kn = {k: n_k[i] for i, k in enumerate(KERNELS)}
+    split, roofs = kernel_table(plan, kms, kn, steps, nsub, pk)
+    gpu_out = np.asfortranarray(out_d.cpu().numpy().T)
+    # end to end: host arrays through the C ABI
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a, np.float32).T)).pin_memory()
+    x0_p, y_p, b_p = pin(x0_h), pin(st.ynoisy), pin(st.background)
+    out_p = torch.empty_like(x0_p).pin_memory()
+    e2e = []
+    for r in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        S.check(L.spect_osem_host(plan.handle, out_p.data_ptr(), x0_p.data_ptr(), y_p.data_ptr(), b_p.data_ptr(),
+                                  nb, niter))
+        if r:
+            e2e.append(time.perf_counter() - t0)
+    res = {"workload": f"{name}: {st.nview} views, {plan.px}x{plan.pz} PSF, "
+                       f"{'ML-EM' if nb == 1 else f'OS-EM {nb} subsets'} x {niter} iterations",
+           "path": "fused projector pair" if plan.fused else "split kernels",
+           "recons_per_s": round(1e3 * steps / float(np.sum(times)), 3), "ms_per_recon": round(float(np.mean(times)), 3),
+           "e2e_recons_per_s": round(len(e2e) / float(np.sum(e2e)), 3),
+           "h2d_bytes": int(4 * (nx * ny * nz + 2 * nx * nz * st.nview)), "d2h_bytes": int(4 * nx * ny * nz),
+           "kernels": roofs, "kernel_split": split}
+    if not args.no_cpu_baseline:
+        if nb == 1:
+            G32 = O.Geometry(st.mumap, st.psfs, st.dy)
+            t0 = time.perf_counter()
+            r32 = G32.mlem(x0_h, st.ynoisy, st.background, niter)
+            t32 = time.perf_counter() - t0
+            r64 = O.Geometry(st.mumap, st.psfs, st.dy, dtype=np.float64).mlem(x0_h, st.ynoisy, st.background, niter)
+            res["cpu_oracle"] = {"recons_per_s": round(1.0 / t32, 5), "cores": os.cpu_count(),
+                                 "sample": "one full ML-EM reconstruction, Float32, measured"}
+            res["parity"] = {"what": "full reconstruction", "max_rel_vs_oracle_f32": float(np.abs(gpu_out - r32).max() / np.abs(r32).max()),
+                             "max_rel_vs_oracle_f64": float(np.abs(gpu_out - r64).max() / np.abs(r64).max())}
+        else:
+            idx = np.arange(0, st.nview, nb, dtype=np.int32)
+            asum_d, x_d = torch.empty_like(x0_d), dev(x0_h)
+            ip = idx.ctypes.data_as(ctypes.c_void_p)
+            S.check(L.spect_subset_sensitivity(plan.handle, asum_d.data_ptr(), ip, len(idx), sp))
+            S.check(L.spect_em_subset_update(plan.handle, x_d.data_ptr(), y_d.data_ptr(), b_d.data_ptr(),
+                                             asum_d.data_ptr(), ip, len(idx), sp))
+            torch.cuda.synchronize()
+            g1 = np.asfortranarray(x_d.cpu().numpy().T)
+            par = {"what": f"one OS-EM subset update (views 0:{nb}:{st.nview}) from a uniform start"}
+            for dt, key in ((np.float32, "max_rel_vs_oracle_f32"), (np.float64, "max_rel_vs_oracle_f64")):
+                G = O.Geometry(st.mumap, st.psfs, st.dy, dtype=dt)
+                ones = np.ones((nx, nz, len(idx)), dt, order="F")
+                a = G.backproject(ones, index=idx)
+                a = np.where(a == 0, np.inf, a)
+                ybar = G.project(x0_h.astype(dt), index=idx)
+                r = st.ynoisy[:, :, idx].astype(dt) / (ybar + st.background[:, :, idx].astype(dt))
+                ref = x0_h.astype(dt) * (G.backproject(np.asfortranarray(r), index=idx) / a)
+                par[key] = float(np.abs(g1 - ref).max() / np.abs(ref).max())
+            res["parity"] = par
+    plan.close()
+    return res
 
 
 def load_workloads():

@@ -95,6 +95,15 @@ int spect_plan_info(spect_plan_t plan, int out[8], size_t* bytes);
  * (1) or the FFT kernels (0).  spect_plan_autotune keeps the faster. */
 int spect_plan_conv_kernels(spect_plan_t plan, int out[4]);
 
+/* 1 in *fused when the plan runs the fused projector pair (rotation,
+ * attenuation, separable PSF convolution and depth sum in one forward kernel;
+ * the adjoint convolution then an atomic-free gather rotation adjoint with
+ * the EM update fused), 0 when it runs the split kernels.  The fused pair is
+ * used for :two plans with the attenuation cache, rank-1 PSF planes and planes
+ * that fit in shared memory (SPECT_ZPATH=0 turns it off).  No counterpart in
+ * the reference (query of this implementation's kernel choice). */
+int spect_plan_fused(spect_plan_t plan, int* fused);
+
 /* project!(views, image, plan; index) (src/project.jl:143-163).
  * views[nindex][nz][nx] = P_{index[i]} image; index NULL = all views in order
  * (nindex must then be nview).  Device pointers, enqueued on stream. */
@@ -226,6 +235,13 @@ int spect_server_destroy(spect_server_t server);
 unsigned long long spect_kernel_launches(void);
 int spect_plan_profile(spect_plan_t plan, int on);
 int spect_plan_kernel_times(spect_plan_t plan, double ms[8], long long counts[8]);
+
+/* FP32 (CUDA-core) peak of the current device, measured: independent FFMA
+ * chains on every SM (4 blocks x 512 threads per SM, 16 chains a thread),
+ * best of 5 timed launches; writes TFLOP/s (2 FLOP per FMA).  The roofline
+ * denominator for this path's FP32-bound kernels (no counterpart in the
+ * reference; measurement support).  Synchronous. */
+int spect_fp32_peak(double* tflops);
 
 /* psf_gauss(; ny, px, pz, fwhm_x, fwhm_z) (src/psf-gauss.jl:24-55): host
  * generator of depth-dependent Gaussian PSFs into psf[ny][pz][px] (Julia

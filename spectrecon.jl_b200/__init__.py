@@ -196,6 +196,15 @@ class SPECTplan:
         return {"forward": name[out[2]], "adjoint": name[out[3]],
                 "direct_forward_ok": bool(out[0]), "direct_adjoint_ok": bool(out[1])}
 
+    @property
+    def fused(self):
+        """True when the plan runs the fused projector pair (rotation,
+        attenuation, separable convolution and depth sum in one forward
+        kernel; gather rotation adjoint with the EM update fused)."""
+        out = ctypes.c_int(0)
+        check(_native.lib().spect_plan_fused(self._h, ctypes.byref(out)))
+        return bool(out.value)
+
     def autotune(self, nindex=None):
         """Time candidate launch shapes for calls with nindex views (default
         nview) and keep the fastest; returns (forward_ms, adjoint_ms)."""

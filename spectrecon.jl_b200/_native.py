@@ -34,6 +34,7 @@ _SIGS = {
     "spect_plan_destroy": ([_P], _I),
     "spect_plan_info": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_Z)], _I),
     "spect_plan_conv_kernels": ([_P, ctypes.POINTER(_I)], _I),
+    "spect_plan_fused": ([_P, ctypes.POINTER(_I)], _I),
     "spect_project": ([_P, _P, _P, _P, _I, _P], _I),
     "spect_project_host": ([_P, _P, _P, _P, _I], _I),
     "spect_project_static_scratch": ([_P, _P, _P, _P, _I, _P], _I),
@@ -56,6 +57,7 @@ _SIGS = {
     "spect_server_stats": ([_P, _P], _I),
     "spect_server_destroy": ([_P], _I),
     "spect_kernel_launches": ([], ctypes.c_ulonglong),
+    "spect_fp32_peak": ([ctypes.POINTER(_D)], _I),
     "spect_plan_profile": ([_P, _I], _I),
     "spect_plan_kernel_times": ([_P, _P, _P], _I),
     "spect_psf_gauss": ([_P, _I, _I, _I, _P, _P], _I),

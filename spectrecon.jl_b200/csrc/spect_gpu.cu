@@ -581,7 +581,7 @@ int zbackward(spect_plan_s* p, float* outIZ, const float* views, const int* vidx
     CUDA_TRY(cudaMemsetAsync(outIZ, 0, sizeof(float) * p->izN, st));
     return SPECT_OK;
   }
-  const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 16, 256));
+  const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 8, 256));  // 8 lanes per image column
   for (int g0 = 0; g0 < nidx; g0 += p->gmax) {
     const int nv = std::min(p->gmax, nidx - g0);
     const int* vi = vidx + g0;
@@ -999,7 +999,7 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
     std::vector<int> fsh, ash;
     for (int i = 0; i < kZNShapes; ++i) {
       const int cap = kZShapes[i].nt * kZShapes[i].nth;
-      if (cap >= xtasks && cap <= 2 * xtasks) fsh.push_back(i);
+      if (cap >= xtasks && cap <= 2 * xtasks && kZShapes[i].nth <= 640) fsh.push_back(i);
       if (kZShapes[i].nt == 1 && kZShapes[i].nth <= 640) ash.push_back(i);
     }
     if (fsh.empty()) fsh.push_back(p->zshape_fwd);
@@ -1320,15 +1320,16 @@ void clamp_tails(const double* w, int p, float* EL, float* ER) {
   }
 }
 
-// zpath launch shapes: forward -- the fewest thread slots holding every x
-// task of a plane (ties: more threads); adjoint -- the least padded x and z
-// passes, one task per thread and pass (no 1024-thread shape: it spills)
+// zpath launch shapes (no 1024-thread shape: it leaves too few registers):
+// forward -- the fewest thread slots holding every x task of a plane (ties:
+// more threads); adjoint -- the least padded x and z passes, one task per
+// thread and pass
 int zpick_fwd(const ZGeom& g) {
   const int xtasks = g.nz * (g.nx / 8);
   int best = -1;
   for (int i = 0; i < kZNShapes; ++i) {
     const int cap = kZShapes[i].nt * kZShapes[i].nth;
-    if (cap < xtasks) continue;
+    if (cap < xtasks || kZShapes[i].nth > 640) continue;  // 1024 threads leave too few registers
     if (best < 0 || cap < kZShapes[best].nt * kZShapes[best].nth ||
         (cap == kZShapes[best].nt * kZShapes[best].nth && kZShapes[i].nth > kZShapes[best].nth))
       best = i;
@@ -1801,6 +1802,12 @@ int spect_plan_conv_kernels(spect_plan_t p, int out[4]) {
   return SPECT_OK;
 }
 
+int spect_plan_fused(spect_plan_t p, int* fused) {
+  if (!p || !fused) return fail(SPECT_ERR_ARG, "null pointer argument");
+  *fused = p->zpath;
+  return SPECT_OK;
+}
+
 int spect_project(spect_plan_t p, float* views, const float* image, const int32_t* index, int nindex, void* stream) {
   if (!p || !views || !image) return fail(SPECT_ERR_ARG, "null pointer argument");
   std::lock_guard<std::mutex> lk(p->mu);
@@ -2053,6 +2060,57 @@ int spect_plan_autotune(spect_plan_t p, int nindex, double ms[2]) {
 
 unsigned long long spect_kernel_launches(void) { return g_launches.load(); }
 
+}  // extern "C"
+
+namespace {
+// independent FMA chains (x <- x a + b), 16 a thread: the FP32 pipe's rate
+__global__ void __launch_bounds__(512) k_fma_chains(float* out, int iters, float a, float b) {
+  float x[16];
+#pragma unroll
+  for (int q = 0; q < 16; ++q) x[q] = threadIdx.x * 1e-3f + q;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int q = 0; q < 16; ++q) x[q] = fmaf(x[q], a, b);
+  float s = 0.f;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) s += x[q];
+  if (s == 12345.f) out[0] = s;  // keeps the chains live
+}
+}  // namespace
+
+extern "C" {
+
+int spect_fp32_peak(double* tflops) {
+  if (!tflops) return fail(SPECT_ERR_ARG, "null pointer argument");
+  int dev = 0, sms = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  float* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, sizeof(float)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int iters = 1 << 15, grid = 4 * sms, thr = 512;
+  float best = 1e30f;
+  cudaError_t e = cudaSuccess;
+  for (int r = 0; r < 6 && e == cudaSuccess; ++r) {  // r = 0: warm-up
+    cudaEventRecord(e0);
+    k_fma_chains<<<grid, thr>>>(d, iters, 0.999f, 0.001f);
+    cudaEventRecord(e1);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && ms > 0.f) best = std::min(best, ms);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string("fp32 peak probe: ") + cudaGetErrorString(e));
+  *tflops = (double)grid * thr * iters * 16 * 2 / (best * 1e-3) / 1e12;
+  return SPECT_OK;
+}
+
 int spect_plan_profile(spect_plan_t p, int on) {
   if (!p) return fail(SPECT_ERR_ARG, "null plan");
   std::lock_guard<std::mutex> lk(p->mu);
@@ -2163,6 +2221,8 @@ struct ServerJob {
   cudaStream_t st = nullptr;
   cudaEvent_t ev = nullptr;
   float *d_x = nullptr, *d_x0 = nullptr, *d_y = nullptr, *d_bg = nullptr;
+  float* h_out = nullptr;  // pinned result (from the server's pool), filled on the job's stream
+  size_t h_cap = 0;
 };
 
 size_t est_job_bytes(const ServerJob& j, bool att) {
@@ -2207,11 +2267,45 @@ struct spect_server_s {
   // job's plan on the host (validation, uploads, PSF spectra) the others
   // keep admitting and retiring
   std::vector<std::thread> workers;
+  // pinned result buffers, reused across jobs (freed at destroy: freeing
+  // pinned memory synchronises the device)
+  std::mutex pool_mu;
+  std::vector<std::pair<float*, size_t>> pool;
 };
 
 namespace {
 
-void job_release(ServerJob* j) {
+// pinned buffer of at least n floats from the pool (or a new one)
+float* pool_get(spect_server_s* S, size_t n, size_t* cap) {
+  {
+    std::lock_guard<std::mutex> lk(S->pool_mu);
+    for (size_t i = 0; i < S->pool.size(); ++i)
+      if (S->pool[i].second >= n) {
+        float* q = S->pool[i].first;
+        *cap = S->pool[i].second;
+        S->pool.erase(S->pool.begin() + i);
+        return q;
+      }
+  }
+  float* q = nullptr;
+  if (cudaMallocHost((void**)&q, sizeof(float) * n) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  *cap = n;
+  return q;
+}
+
+void pool_put(spect_server_s* S, float* q, size_t cap) {
+  if (!q) return;
+  std::lock_guard<std::mutex> lk(S->pool_mu);
+  S->pool.push_back({q, cap});
+}
+
+// releases a finished job's device resources (stream-ordered frees on its
+// stream; the stream is destroyed once its queued work has run) and returns
+// its pinned buffer to the pool; no device-wide synchronisation
+void job_release(spect_server_s* S, ServerJob* j) {
   if (j->plan) free_plan(j->plan);  // stream-ordered frees on the job's stream
   j->plan = nullptr;
   float* bufs[] = {j->d_x, j->d_x0, j->d_y, j->d_bg};
@@ -2222,6 +2316,9 @@ void job_release(ServerJob* j) {
   if (j->st) cudaStreamDestroy(j->st);  // released once its queued frees ran
   j->ev = nullptr;
   j->st = nullptr;
+  pool_put(S, j->h_out, j->h_cap);
+  j->h_out = nullptr;
+  j->h_cap = 0;
   std::vector<float>().swap(j->mumap);
   std::vector<float>().swap(j->psfs);
   std::vector<float>().swap(j->y);
@@ -2229,7 +2326,7 @@ void job_release(ServerJob* j) {
   std::vector<float>().swap(j->x0);
 }
 
-int job_admit(ServerJob* j, size_t budget) {
+int job_admit(spect_server_s* S, ServerJob* j, size_t budget) {
   CUDA_TRY(cudaStreamCreateWithFlags(&j->st, cudaStreamNonBlocking));
   CUDA_TRY(cudaEventCreateWithFlags(&j->ev, cudaEventDisableTiming));
   PlanOpts o;
@@ -2255,6 +2352,10 @@ int job_admit(ServerJob* j, size_t budget) {
   CUDA_TRY(cudaMemcpyAsync(j->d_bg, j->bg.data(), sizeof(float) * V, cudaMemcpyHostToDevice, j->st));
   STATUS_TRY(prepare_osem(plan, j->nblocks, j->niter));
   STATUS_TRY(enqueue_osem(plan, j->d_x, j->d_x0, j->d_y, j->d_bg, j->nblocks, j->niter, j->st));
+  // the result lands in pinned memory before the completion event
+  j->h_out = pool_get(S, N, &j->h_cap);
+  if (!j->h_out) return fail(SPECT_ERR_OOM, "pinned result buffer");
+  CUDA_TRY(cudaMemcpyAsync(j->h_out, j->d_x, sizeof(float) * N, cudaMemcpyDeviceToHost, j->st));
   CUDA_TRY(cudaEventRecord(j->ev, j->st));
   j->bytes = std::max(plan->bytes, j->est);  // conservative accounting
   return SPECT_OK;
@@ -2262,49 +2363,44 @@ int job_admit(ServerJob* j, size_t budget) {
 
 void server_loop(spect_server_s* S) {
   cudaSetDevice(S->device);
-  float* staging = nullptr;  // this thread's pinned result staging
-  size_t staging_n = 0;
   std::unique_lock<std::mutex> lk(S->mu);
+  std::vector<std::pair<ServerJob*, cudaError_t>> finished;
   for (;;) {
-    // completions
+    // completions: poll the events (non-blocking) under the lock, then copy
+    // the pinned results and release the jobs outside it
+    finished.clear();
     for (size_t i = 0; i < S->active.size();) {
       ServerJob* j = S->active[i];
-      cudaError_t q = cudaEventQuery(j->ev);
+      const cudaError_t q = cudaEventQuery(j->ev);
       if (q == cudaErrorNotReady) {
         ++i;
         continue;
       }
-      const size_t N = j->plan ? j->plan->N : 0;
-      if (q == cudaSuccess) {
-        if (staging_n < N) {
-          if (staging) cudaFreeHost(staging);
-          staging = nullptr;
-          staging_n = 0;
-          if (cudaMallocHost((void**)&staging, sizeof(float) * N) == cudaSuccess) staging_n = N;
-        }
-        cudaError_t e = staging ? cudaMemcpyAsync(staging, j->d_x, sizeof(float) * N, cudaMemcpyDeviceToHost, j->st)
-                                : cudaErrorMemoryAllocation;
-        if (e == cudaSuccess) e = cudaStreamSynchronize(j->st);
-        if (e == cudaSuccess) {
-          j->result.assign(staging, staging + N);
+      finished.push_back({j, q});
+      S->used -= std::min(S->used, j->bytes);
+      S->active.erase(S->active.begin() + i);
+    }
+    if (!finished.empty()) {
+      lk.unlock();
+      for (auto& f : finished) {
+        ServerJob* j = f.first;
+        if (f.second == cudaSuccess) j->result.assign(j->h_out, j->h_out + j->plan->N);
+        j->t_done = Clock::now();
+        job_release(S, j);
+      }
+      lk.lock();
+      for (auto& f : finished) {
+        ServerJob* j = f.first;
+        if (f.second == cudaSuccess) {
           j->state = 2;
           S->n_done++;
         } else {
           j->state = 3;
           j->status = SPECT_ERR_CUDA;
-          j->err = std::string("result copy: ") + cudaGetErrorString(e);
+          j->err = std::string("job execution: ") + cudaGetErrorString(f.second);
           S->n_failed++;
         }
-      } else {
-        j->state = 3;
-        j->status = SPECT_ERR_CUDA;
-        j->err = std::string("job execution: ") + cudaGetErrorString(q);
-        S->n_failed++;
       }
-      j->t_done = Clock::now();
-      S->used -= std::min(S->used, j->bytes);
-      job_release(j);
-      S->active.erase(S->active.begin() + i);
       S->cv_done.notify_all();
     }
     // admissions (FIFO) while slots and memory allow
@@ -2326,15 +2422,18 @@ void server_loop(spect_server_s* S) {
       S->used += j->est;
       lk.unlock();
       j->t_admit = Clock::now();
-      int rc = job_admit(j, S->budget);
+      const int rc = job_admit(S, j, S->budget);
+      std::string err = rc == SPECT_OK ? std::string() : g_err;
+      if (rc != SPECT_OK) {
+        j->t_done = Clock::now();
+        job_release(S, j);
+      }
       lk.lock();
       S->used -= j->est;
       if (rc != SPECT_OK) {
         j->state = 3;
         j->status = rc;
-        j->err = g_err;
-        j->t_done = Clock::now();
-        job_release(j);
+        j->err = err;
         S->n_failed++;
         S->cv_done.notify_all();
         continue;
@@ -2353,8 +2452,6 @@ void server_loop(spect_server_s* S) {
       lk.lock();
     }
   }
-  lk.unlock();
-  if (staging) cudaFreeHost(staging);
 }
 
 }  // namespace
@@ -2481,6 +2578,7 @@ int spect_server_destroy(spect_server_t S) {
   for (auto& w : S->workers)
     if (w.joinable()) w.join();  // running jobs finish first
   for (auto& kv : S->jobs) delete kv.second;
+  for (auto& b : S->pool) cudaFreeHost(b.first);
   delete S;
   return SPECT_OK;
 }

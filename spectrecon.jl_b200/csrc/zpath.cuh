@@ -27,8 +27,8 @@
 //          plane the x pass and z pass of fft_conv_adj! (src/fft_convolve.jl:
 //          82-130) of the view, times the attenuation, stored as T.
 // k_zrot_adj  imrotate_adj! :two (src/rotatez.jl:390-416) and the view sum
-//          (src/backproject.jl:146-153): output-stationary gather.  A half-warp
-//          owns one image column (x, y) over all z (16 lanes x ZPL values) and
+//          (src/backproject.jl:146-153): output-stationary gather.  A group of
+//          8 lanes owns one image column (x, y) over all z (8 lanes x ZPL) and
 //          sums, over the group's views in order, the bilinear weights of the
 //          rotated-grid points whose footprint covers it: the exact transpose
 //          of the forward sampling, without atomics.  The EM update
@@ -70,25 +70,30 @@ __device__ __forceinline__ void zfma8(const float* __restrict__ w, float4 p, flo
     for (int k = 0; k < 8; ++k) o[k] = fmaf(ws[s], e[s + k], o[k]);
 }
 
-// one 8-output task over a padded line: o[k] += sum_{m < len} w[m] line[k + m]
-// (len a multiple of 8; line and w 16-byte aligned; reads line[0, len + 8))
-__device__ __forceinline__ void zpass8(const float* __restrict__ w, int len, const float* line, float (&o)[8]) {
+// one 8-output task over a zero-padded line, the window in nblk blocks of 8
+// taps (nblk <= 9): o[k] += sum_{m < 8 nblk} w[m] line[k + m] (line and w
+// 16-byte aligned; reads line[0, 8 nblk + 8)).  Fully unrolled with a uniform
+// early exit: the window registers alternate by name, with no loop counter
+// or register moves.
+__device__ __forceinline__ void zpassu(const float* __restrict__ w, int nblk, const float* line, float (&o)[8]) {
   float4 a = ld4(line), b = ld4(line + 4), c, d;
-  int m0 = 0;
-  for (; m0 + 16 <= len; m0 += 16) {
-    c = ld4(line + m0 + 8);
-    d = ld4(line + m0 + 12);
-    zfma8(w + m0, a, b, c, d, o);
-    a = ld4(line + m0 + 16);
-    b = ld4(line + m0 + 20);
-    zfma8(w + m0 + 8, c, d, a, b, o);
-  }
-  if (m0 < len) {
-    c = ld4(line + m0 + 8);
-    d = ld4(line + m0 + 12);
-    zfma8(w + m0, a, b, c, d, o);
+#pragma unroll
+  for (int k = 0; k < 10; k += 2) {
+    if (k >= nblk) break;
+    c = ld4(line + 8 * k + 8);
+    d = ld4(line + 8 * k + 12);
+    zfma8(w + 8 * k, a, b, c, d, o);
+    if (k + 1 >= nblk) break;
+    a = ld4(line + 8 * k + 16);
+    b = ld4(line + 8 * k + 20);
+    zfma8(w + 8 * k + 8, c, d, a, b, o);
   }
 }
+
+// q = t / n for 0 <= t < 2^20, 1 <= n <= 4096, with r = 1/n rounded to float:
+// (t + 1/2) / n is at least 1/(2n) from an integer, far above the rounding
+// error of (t + 1/2) * r, so truncation gives the exact quotient
+__device__ __forceinline__ int zdiv(int t, float r) { return (int)(((float)t + 0.5f) * r); }
 
 // ------------------------------------------------------------------------
 // Layout changes between the caller's image [z][y][x] and IZ.
@@ -235,6 +240,9 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
   const int nzb = (nz + 7) / 8, ztasks = nx * nzb, nz4 = (nz + 3) / 4, units = nx * nz4;
   const int xtasks = nz * (nx / 8);
   const size_t Lz = (size_t)g.L * nzp;
+  const int ast = g.ast, bs = g.bs, R0 = g.R0, C0 = g.C0, hz = g.hz, hx = g.hx;
+  const int zblk = g.zpw / 8, xblk = g.xpw / 8, zpw = g.zpw;
+  const float rnx = 1.0f / nx, rnz = 1.0f / nz, rnz4 = 1.0f / nz4;
   unsigned phase = 0;
   int yb = 0;  // working-weight buffer of the current plane
   float acc[NT][8];
@@ -293,7 +301,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
       }
       // rotated, attenuated plane into ZB (column x, rows R0 + z), four z at a time
       for (int u = tid; u < units; u += NTH) {
-        const int x = u / nz4, zg = u - x * nz4;
+        const int x = zdiv(u, rnz4), zg = u - x * nz4;
         const float4 w = geoW[x];
         const float* p = a.img + geoO[x] + 4 * zg;
         const float4 t0 = ld4(p), t1 = ld4(p + nzp), t2 = ld4(p + Lz), t3 = ld4(p + Lz + nzp);
@@ -303,7 +311,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         o.y = __fmul_rn(fmaf(w.w, t3.y, fmaf(w.z, t2.y, fmaf(w.y, t1.y, __fmul_rn(w.x, t0.y)))), at.y);
         o.z = __fmul_rn(fmaf(w.w, t3.z, fmaf(w.z, t2.z, fmaf(w.y, t1.z, __fmul_rn(w.x, t0.z)))), at.z);
         o.w = __fmul_rn(fmaf(w.w, t3.w, fmaf(w.z, t2.w, fmaf(w.y, t1.w, __fmul_rn(w.x, t0.w)))), at.w);
-        st4(ZB + (size_t)x * g.ast + g.R0 + 4 * zg, o);
+        st4(ZB + x * ast + R0 + 4 * zg, o);
       }
       __syncthreads();
       if (tid == 0) {  // next plane of this block into the staging buffers
@@ -312,55 +320,56 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
       }
       // z pass: task (x, z block) -> XB rows z, column C0 + x
       const float* ELz = Hw + hs;
-      const float* ERz = ELz + g.hz;
+      const float* ERz = ELz + hz;
       for (int t = tid; t < ztasks; t += NTH) {
-        const int zb = t / nx, x = t - zb * nx, z0 = 8 * zb;
+        const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = 8 * zb;
         float o[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) o[k] = 0.f;
-        const float* col = ZB + (size_t)x * g.ast;
-        zpass8(Hw, g.zpw, col + z0, o);
-        if (z0 < g.hz) {  // clamped rows above the plane
-          const float e0 = col[g.R0];
+        const float* col = ZB + x * ast;
+        zpassu(Hw, zblk, col + z0, o);
+        if (z0 < hz) {  // clamped rows above the plane
+          const float e0 = col[R0];
 #pragma unroll
           for (int k = 0; k < 8; ++k)
-            if (z0 + k < g.hz) o[k] = fmaf(ELz[z0 + k], e0, o[k]);
+            if (z0 + k < hz) o[k] = fmaf(ELz[z0 + k], e0, o[k]);
         }
-        if (z0 + 8 > nz - g.hz) {  // clamped rows below
-          const float e1 = col[g.R0 + nz - 1];
+        if (z0 + 8 > nz - hz) {  // clamped rows below
+          const float e1 = col[R0 + nz - 1];
 #pragma unroll
           for (int k = 0; k < 8; ++k) {
             const int kk = nz - 1 - z0 - k;
-            if (kk >= 0 && kk < g.hz) o[k] = fmaf(ERz[kk], e1, o[k]);
+            if (kk >= 0 && kk < hz) o[k] = fmaf(ERz[kk], e1, o[k]);
           }
         }
+        float* xo = XB + z0 * bs + C0 + x;
 #pragma unroll
         for (int k = 0; k < 8; ++k)
-          if (z0 + k < nz) XB[(size_t)(z0 + k) * g.bs + g.C0 + x] = o[k];
+          if (z0 + k < nz) xo[k * bs] = o[k];
       }
       __syncthreads();
       // x pass, accumulated over the chunk
-      const float* ELx = ERz + g.hz;
-      const float* ERx = ELx + g.hx;
+      const float* ELx = ERz + hz;
+      const float* ERx = ELx + hx;
 #pragma unroll
       for (int i = 0; i < NT; ++i) {
         const int t = tid + i * NTH;
         if (t < xtasks) {
-          const int xb = t / nz, z = t - xb * nz, x0 = 8 * xb;
-          const float* row = XB + (size_t)z * g.bs;
-          zpass8(Hw + g.zpw, g.xpw, row + x0, acc[i]);
-          if (x0 < g.hx) {
-            const float e0 = row[g.C0];
+          const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
+          const float* row = XB + z * bs;
+          zpassu(Hw + zpw, xblk, row + x0, acc[i]);
+          if (x0 < hx) {
+            const float e0 = row[C0];
 #pragma unroll
             for (int k = 0; k < 8; ++k)
-              if (x0 + k < g.hx) acc[i][k] = fmaf(ELx[x0 + k], e0, acc[i][k]);
+              if (x0 + k < hx) acc[i][k] = fmaf(ELx[x0 + k], e0, acc[i][k]);
           }
-          if (x0 + 8 > nx - g.hx) {
-            const float e1 = row[g.C0 + nx - 1];
+          if (x0 + 8 > nx - hx) {
+            const float e1 = row[C0 + nx - 1];
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
               const int kk = nx - 1 - x0 - k;
-              if (kk < g.hx) acc[i][k] = fmaf(ERx[kk], e1, acc[i][k]);
+              if (kk < hx) acc[i][k] = fmaf(ERx[kk], e1, acc[i][k]);
             }
           }
         }
@@ -373,7 +382,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
     for (int i = 0; i < NT; ++i) {
       const int t = tid + i * NTH;
       if (t < xtasks) {
-        const int xb = t / nz, z = t - xb * nz;
+        const int xb = zdiv(t, rnz), z = t - xb * nz;
         float* o = out + (size_t)z * nx + 8 * xb;
         st4(o, make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]));
         st4(o + 4, make_float4(acc[i][4], acc[i][5], acc[i][6], acc[i][7]));
@@ -438,6 +447,9 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   next(qi, qy);  // P2: the next plane to issue
   if (!((int)blockIdx.x < nitems)) return;
   const int nzb = (nz + 7) / 8, ztasks = nx * nzb, xtasks = nz * (nx / 8);
+  const int ast = g.ast, bs = g.bs, R0 = g.R0, C0 = g.C0, hz = g.hz, hx = g.hx;
+  const int zblk = g.zpw / 8, xblk = g.xpw / 8;
+  const float rnx = 1.0f / nx, rnz = 1.0f / nz;
   unsigned phases = 0u;
   int b = 0;
   for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
@@ -471,43 +483,43 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 #pragma unroll
       for (int i = 0; i < NT; ++i)
         for (int t = tid + i * NTH; t < xtasks; t += NT * NTH) {
-          const int xb = t / nz, z = t - xb * nz, x0 = 8 * xb;
-          const float* row = VB + (size_t)z * g.bs;
+          const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
+          const float* row = VB + z * bs;
           float o[8];
 #pragma unroll
           for (int k = 0; k < 8; ++k) o[k] = 0.f;
-          zpass8(ax, g.xpw, row + x0, o);
+          zpassu(ax, xblk, row + x0, o);
           if (x0 == 0)
-            for (int k = 0; k < g.hx; ++k) o[0] = fmaf(cLx[k], row[g.C0 + k], o[0]);
+            for (int k = 0; k < hx; ++k) o[0] = fmaf(cLx[k], row[C0 + k], o[0]);
           if (x0 + 8 == nx)
-            for (int k = 0; k < g.hx; ++k) o[7] = fmaf(cRx[k], row[g.C0 + nx - 1 - k], o[7]);
-          float* w = WB + (size_t)x0 * g.ast + g.R0 + z;
+            for (int k = 0; k < hx; ++k) o[7] = fmaf(cRx[k], row[C0 + nx - 1 - k], o[7]);
+          float* w = WB + x0 * ast + R0 + z;
 #pragma unroll
-          for (int k = 0; k < 8; ++k) w[(size_t)k * g.ast] = o[k];
+          for (int k = 0; k < 8; ++k) w[k * ast] = o[k];
         }
       __syncthreads();
       // z pass: task (x, z block) -> T column (x, y) of the slot
       const float* attv = a.att + (((size_t)v * ny + y) * nx) * nzp;
       float* Tp = a.T + (((size_t)slot * ny + y) * nx) * nzp;
       for (int t = tid; t < ztasks; t += NTH) {
-        const int zb = t / nx, x = t - zb * nx, z0 = 8 * zb;
-        const float4 a0 = ld4(attv + (size_t)x * nzp + z0), a1 = ld4(attv + (size_t)x * nzp + z0 + 4);
-        const float* col = WB + (size_t)x * g.ast;
+        const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = 8 * zb;
+        const float4 a0 = ld4(attv + x * nzp + z0), a1 = ld4(attv + x * nzp + z0 + 4);
+        const float* col = WB + x * ast;
         float o[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) o[k] = 0.f;
-        zpass8(az, g.zpw, col + z0, o);
+        zpassu(az, zblk, col + z0, o);
         if (z0 == 0)
-          for (int k = 0; k < g.hz; ++k) o[0] = fmaf(cLz[k], col[g.R0 + k], o[0]);
+          for (int k = 0; k < hz; ++k) o[0] = fmaf(cLz[k], col[R0 + k], o[0]);
         if (z0 <= nz - 1 && nz - 1 < z0 + 8) {
           const int kz = nz - 1 - z0;
           float s = 0.f;
-          for (int k = 0; k < g.hz; ++k) s = fmaf(cRz[k], col[g.R0 + nz - 1 - k], s);
+          for (int k = 0; k < hz; ++k) s = fmaf(cRz[k], col[R0 + nz - 1 - k], s);
 #pragma unroll
           for (int k = 0; k < 8; ++k)
             if (k == kz) o[k] += s;
         }
-        float* dst = Tp + (size_t)x * nzp + z0;
+        float* dst = Tp + x * nzp + z0;
         st4(dst, make_float4(__fmul_rn(a0.x, o[0]), __fmul_rn(a0.y, o[1]), __fmul_rn(a0.z, o[2]),
                              __fmul_rn(a0.w, o[3])));
         st4(dst + 4, make_float4(__fmul_rn(a1.x, o[4]), __fmul_rn(a1.y, o[5]), __fmul_rn(a1.z, o[6]),
@@ -522,13 +534,15 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 }
 
 // ------------------------------------------------------------------------
-// k_zrot_adj<ZPL>: half-warp h owns image column p = (j1, j2) (grid-stride),
-// lane l the z values l + 16 q, q < ZPL (nzp = 16 ZPL).  For every slot s in
-// order, the rotated-grid points (x, y) whose bilinear footprint contains
-// (j1, j2) -- those with floor(s1) in {j1-1, j1} and floor(s2) in {j2-1, j2}
-// -- lie within |cos| + |sin| of the inverse-rotated pixel centre, so the
-// candidates are at most 3 x 3 points; each is tested with the forward's own
-// position arithmetic and weighted with the forward's weight product.
+// k_zrot_adj<ZPL>: an 8-lane group owns image column p = (j1, j2)
+// (grid-stride), lane l the z values l + 8 q, q < ZPL (nzp = 8 ZPL): one
+// 32-byte sector per lane group and load, and the candidate geometry shared
+// by the group's 8 lanes (4 columns per warp).  For every slot s in order,
+// the rotated-grid points (x, y) whose bilinear footprint contains (j1, j2)
+// -- those with floor(s1) in {j1-1, j1} and floor(s2) in {j2-1, j2} -- lie
+// within |cos| + |sin| of the inverse-rotated pixel centre, so the candidates
+// are at most 3 x 3 points; each is tested with the forward's own position
+// arithmetic and weighted with the forward's weight product.
 // Epilogue (IZ layout): v = acc (+ prev); mode 1: zeros -> +Inf; mode 2:
 // v = x * (v / asum); out = v (z < nz only; out may be prev or x).
 template <int ZPL>
@@ -536,11 +550,11 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
                                                  const float4* __restrict__ rot, const int* __restrict__ vidx, int nv,
                                                  const float* prev, float* out, const float* x,
                                                  const float* __restrict__ asum, int mode) {
-  const int lane = threadIdx.x & 15;
-  const int nhw = (gridDim.x * blockDim.x) >> 4;
+  const int lane = threadIdx.x & 7;
+  const int ngr = (gridDim.x * blockDim.x) >> 3;
   const int nx = g.nx, ny = g.ny, nzp = g.nzp;
   const float c0 = g.c0;
-  for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; p < nx * nx; p += nhw) {
+  for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; p < nx * nx; p += ngr) {
     const int j2 = p / nx, j1 = p - j2 * nx;
     const float fj1 = (float)j1, fj2 = (float)j2;
     float acc[ZPL];
@@ -576,7 +590,7 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
             const float w = __fmul_rn(a1, a2);
             const float* tp = Ts + ((size_t)yy * nx + xx) * nzp;
 #pragma unroll
-            for (int q = 0; q < ZPL; ++q) acc[q] = fmaf(w, tp[16 * q], acc[q]);
+            for (int q = 0; q < ZPL; ++q) acc[q] = fmaf(w, tp[8 * q], acc[q]);
           }
         }
       }
@@ -584,12 +598,12 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
     const size_t o = ((size_t)(j2 + g.pad) * g.L + j1 + g.pad) * nzp + lane;
 #pragma unroll
     for (int q = 0; q < ZPL; ++q) {
-      if (lane + 16 * q < g.nz) {
+      if (lane + 8 * q < g.nz) {
         float v = acc[q];
-        if (prev) v += prev[o + 16 * q];
+        if (prev) v += prev[o + 8 * q];
         if (mode == 1 && v == 0.f) v = __int_as_float(0x7f800000);
-        if (mode == 2) v = x[o + 16 * q] * (v / asum[o + 16 * q]);
-        out[o + 16 * q] = v;
+        if (mode == 2) v = x[o + 8 * q] * (v / asum[o + 8 * q]);
+        out[o + 8 * q] = v;
       }
     }
   }

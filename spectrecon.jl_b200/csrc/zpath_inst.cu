@@ -44,11 +44,11 @@ cudaError_t zadj_launch(int shape, int grid, size_t smem, cudaStream_t st, const
 cudaError_t zrot_adj_launch(const ZGeom& g, int grid, cudaStream_t st, const float* T, const float4* rot,
                             const int* vidx, int nv, const float* prev, float* out, const float* x, const float* asum,
                             int mode) {
-  switch (g.nzp / 16) {
+  switch (g.nzp / 8) {  // nzp is a multiple of 16
 #define ZCASE(n) \
   case n: return zrot<n>(g, grid, st, T, rot, vidx, nv, prev, out, x, asum, mode);
-    ZCASE(1) ZCASE(2) ZCASE(3) ZCASE(4) ZCASE(5) ZCASE(6) ZCASE(7) ZCASE(8)
-    ZCASE(9) ZCASE(10) ZCASE(11) ZCASE(12) ZCASE(13) ZCASE(14) ZCASE(15) ZCASE(16)
+    ZCASE(2) ZCASE(4) ZCASE(6) ZCASE(8) ZCASE(10) ZCASE(12) ZCASE(14) ZCASE(16)
+    ZCASE(18) ZCASE(20) ZCASE(22) ZCASE(24) ZCASE(26) ZCASE(28) ZCASE(30) ZCASE(32)
 #undef ZCASE
   }
   return cudaErrorInvalidValue;

@@ -75,3 +75,51 @@ def test_static_scratch_rejects_oversized_plan(S):
     assert rc == SPECT_ERR_UNSUPPORTED
     assert "static limit" in L.spect_last_error().decode()
     plan.close()
+
+
+@pytest.mark.parametrize("case,env", [("one", {}), ("gauss-fused", {}), ("gauss-split-direct", {"SPECT_ZPATH": "0"}),
+                                      ("gauss-fft", {"SPECT_CONV": "fft"})])
+def test_static_scratch_kernel_paths(S, O, monkeypatch, case, env):
+    """Every kernel path through the static array -- the :one shear rotation,
+    the fused projector pair (Gaussian, hence separable, PSFs), the split
+    direct-convolution kernels and the FFT kernels -- gives spect_project's
+    result on two calls in a row, and the oracle's within the parity
+    tolerance."""
+    import torch
+
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    rng = np.random.default_rng(11)
+    nx, nz, nview = 64, 32, 8
+    mumap = np.asfortranarray(0.01 * rng.random((nx, nx, nz)), np.float32)
+    if case == "one":
+        psfs = sym_psfs(rng, 9, 7, nx, nview)
+        plan = S.SPECTplan(mumap, psfs, 4.8, interpmeth="one")
+    else:
+        psfs = np.asfortranarray(np.repeat(S.psf_gauss(ny=nx, px=11, fwhm_start=1, fwhm_end=3)[:, :, :, None],
+                                           nview, axis=3))
+        plan = S.SPECTplan(mumap, psfs, 4.8)
+    assert plan.fused == (case == "gauss-fused")
+    L = S._native.lib()
+    x = rng.random((nx, nx, nz)).astype(np.float32)
+    image = _dev(torch, x)
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    index = np.array([5, 0, 3, 6], np.int32)
+    ip = index.ctypes.data_as(ctypes.c_void_p)
+    ref = torch.empty((len(index), nz, nx), device="cuda")
+    S.check(L.spect_project(plan.handle, ref.data_ptr(), image.data_ptr(), ip, len(index), sp))
+    outs = []
+    for _ in range(2):
+        out = torch.full((len(index), nz, nx), float("nan"), device="cuda")
+        S.check(L.spect_project_static_scratch(plan.handle, out.data_ptr(), image.data_ptr(), ip, len(index), sp))
+        outs.append(out)
+    torch.cuda.synchronize()
+    r = ref.cpu().numpy()
+    G = O.Geometry(mumap, psfs, 4.8, interp="one" if case == "one" else "two")
+    want = np.ascontiguousarray(G.project(x, index=index).T)  # [view][z][x]
+    for out in outs:
+        o = out.cpu().numpy()
+        assert np.isfinite(o).all()
+        assert relerr(o, r) <= TOL
+        assert relerr(o, want) <= TOL
+    plan.close()
