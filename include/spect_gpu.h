@@ -37,16 +37,16 @@ extern "C" {
 /* status codes; messages mirror the reference's throws */
 enum {
   SPECT_OK = 0,
-  SPECT_ERR_NX_NE_NY = 1,      /* "nx != ny"            src/spectplan.jl:76 (98 in file) */
-  SPECT_ERR_NX_ODD = 2,        /* "nx odd"              src/spectplan.jl:77 (99) */
-  SPECT_ERR_PSF_NOT_ODD = 3,   /* "non-odd size psfs"   src/spectplan.jl:82 (104) */
-  SPECT_ERR_PSF_ASYM = 4,      /* "asym. psf"           src/spectplan.jl:83-84 (105-106) */
-  SPECT_ERR_INTERP = 5,        /* "bad interpmeth"      src/spectplan.jl:87 (109) */
-  SPECT_ERR_NTHREAD = 6,       /* "bad nthread"         src/spectplan.jl:90 (112) */
-  SPECT_ERR_MODE = 7,          /* "bad mode"            src/spectplan.jl:93 (115) */
+  SPECT_ERR_NX_NE_NY = 1,      /* "nx != ny"            src/spectplan.jl:76 */
+  SPECT_ERR_NX_ODD = 2,        /* "nx odd"              src/spectplan.jl:77 */
+  SPECT_ERR_PSF_NOT_ODD = 3,   /* "non-odd size psfs"   src/spectplan.jl:82 */
+  SPECT_ERR_PSF_ASYM = 4,      /* "asym. psf"           src/spectplan.jl:83-84 */
+  SPECT_ERR_INTERP = 5,        /* "bad interpmeth"      src/spectplan.jl:87 */
+  SPECT_ERR_NTHREAD = 6,       /* "bad nthread"         src/spectplan.jl:90 */
+  SPECT_ERR_MODE = 7,          /* "bad mode"            src/spectplan.jl:93 */
   SPECT_ERR_DIM = 8,           /* DimensionMismatch     src/project.jl:204-205, src/ml-os-em.jl:25-26 */
-  SPECT_ERR_BACKGROUND = 9,    /* "need background > 0" src/ml-os-em.jl:30,106 (324,400) */
-  SPECT_ERR_NBLOCKS = 10,      /* "nview must be divisible by nblocks!" src/ml-os-em.jl:73 (367) */
+  SPECT_ERR_BACKGROUND = 9,    /* "need background > 0" src/ml-os-em.jl:30,106 */
+  SPECT_ERR_NBLOCKS = 10,      /* "nview must be divisible by nblocks!" src/ml-os-em.jl:73 */
   SPECT_ERR_INDEX = 11,        /* view index out of 0..nview-1 (Julia BoundsError) */
   SPECT_ERR_ARG = 12,          /* null pointer / non-positive size */
   SPECT_ERR_UNSUPPORTED = 13,  /* size beyond this build's kernel limits */
@@ -70,7 +70,7 @@ const char* spect_last_error(void);
 int spect_device_info(int* sm_count, size_t* total_mem);
 
 /* SPECTplan(mumap, psfs, dy; T, viewangle, interpmeth, nthread, mode)
- * (src/spectplan.jl:58-137; 80-159 in file).  mumap and psfs are HOST arrays;
+ * (src/spectplan.jl:58-137).  mumap and psfs are HOST arrays;
  * they are validated exactly as the reference does (nx == ny, nx even, px/pz
  * odd, every psfs[:,:,y,v] point-symmetric, interpmeth, nthread == nthreads,
  * mode), uploaded, and the PSF spectra are precomputed on the device.  Unlike
@@ -132,15 +132,13 @@ int spect_project_host(spect_plan_t plan, float* views, const float* image, cons
 int spect_project_static_scratch(spect_plan_t plan, float* views, const float* image, const int32_t* index,
                                  int nindex, void* stream);
 
-/* backproject!(image, views, plan; index) (src/backproject.jl:132-162; 340-370
- * in file).  image = sum_i P_{index[i]}' views[i]; image need not be zeroed. */
+/* backproject!(image, views, plan; index) (src/backproject.jl:132-162).  image = sum_i P_{index[i]}' views[i]; image need not be zeroed. */
 int spect_backproject(spect_plan_t plan, float* image, const float* views, const int32_t* index,
                       int nindex, void* stream);
 int spect_backproject_host(spect_plan_t plan, float* image, const float* views, const int32_t* index,
                            int nindex);
 
-/* mlem!(out, x0, ynoisy, background, A; niter) (src/ml-os-em.jl:21-49;
- * 315-343 in file) with A the plan's full projector.  Device pointers; the
+/* mlem!(out, x0, ynoisy, background, A; niter) (src/ml-os-em.jl:21-49) with A the plan's full projector.  Device pointers; the
  * EM ratio is fused into the forward reduction and the multiplicative update
  * into the back-projection's last stage. */
 int spect_mlem(spect_plan_t plan, float* out, const float* x0, const float* ynoisy,
@@ -149,14 +147,14 @@ int spect_mlem_host(spect_plan_t plan, float* out, const float* x0, const float*
                     const float* background, int niter);
 
 /* osem!(out, x0, ynoisy, background, Ablock(plan, nblocks); niter)
- * (src/ml-os-em.jl:70-131; 364-425 in file): subsets nb:nblocks:nview. */
+ * (src/ml-os-em.jl:70-131): subsets nb:nblocks:nview. */
 int spect_osem(spect_plan_t plan, float* out, const float* x0, const float* ynoisy,
                const float* background, int nblocks, int niter, void* stream);
 int spect_osem_host(spect_plan_t plan, float* out, const float* x0, const float* ynoisy,
                     const float* background, int nblocks, int niter);
 
 /* One fused OS-EM subset update on device buffers (the loop body of
- * src/ml-os-em.jl:123-127; 417-421 in file):
+ * src/ml-os-em.jl:120-127):
  *   x .*= A_s' (y_s ./ (A_s x + b_s)) ./ asum
  * y and background are the FULL [nview][nz][nx] arrays; the subset is
  * index[0..nindex).  asum is A_s' 1 with zeros replaced by +Inf. */

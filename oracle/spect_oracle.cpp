@@ -16,11 +16,11 @@
 //   imrotate!/imrotate_adj! (:one)               src/rotatez.jl:240-322
 //   imrotate!/imrotate_adj! (:two)               src/rotatez.jl:331-416
 //   project! (per view, multi-view :fast)        src/project.jl:77-163
-//   backproject! (per view, multi-view :fast)    src/backproject.jl:277-370
+//   backproject! (per view, multi-view :fast)    src/backproject.jl:69-162
 //   spawner                                      src/spawn.jl:10-17
 //   mlem!, osem!, Ablock subsets                 src/ml-os-em.jl:21-131
-//   viewangle default                            src/spectplan.jl:63 (85 in file)
-//   PlanRotate padsize                           src/plan-rotate.jl:56 (235 in file)
+//   viewangle default                            src/spectplan.jl:63
+//   PlanRotate padsize                           src/plan-rotate.jl:56
 //
 // Third-party arithmetic restated from its published definition:
 //   * FFTW (FFTW.jl, compat "1"): unnormalised forward DFT with exp(-2*pi*i*k*n/N),
@@ -598,7 +598,7 @@ struct Plan {
       for (int n = 0; n < nz; ++n)
         for (int m = 0; m < nx; ++m) view[m + (size_t)n * nx] += A[m + nx * (y + (size_t)ny * n)];
   }
-  // backproject!(image, view, plan, buffer_id, viewidx) (src/backproject.jl:277-332)
+  // backproject!(image, view, plan, buffer_id, viewidx) (src/backproject.jl:69-124)
   void backproject_view(T* image, const T* view, int b, int v) {
     size_t slice = (size_t)nx * ny;
     T* R = imgr[b].data();
@@ -625,7 +625,7 @@ struct Plan {
       project_view(views + (size_t)ii * nx * nz, image, b, index[ii]);
     });
   }
-  // backproject!(image, views, plan; index) :fast (src/backproject.jl:340-370)
+  // backproject!(image, views, plan; index) :fast (src/backproject.jl:132-162)
   void backproject(T* image, const T* views, const int* index, int nidx) {
     size_t N = (size_t)nx * ny * nz;
     std::fill(image, image + N, T(0));

@@ -293,8 +293,8 @@ def project(image, plan_or_mumap, psfs=None, dy=None, interpmeth="two", mode="fa
 
 
 def backproject(views, plan_or_mumap, psfs=None, dy=None, interpmeth="two", mode="fast", index=None, **kw):
-    """``backproject(views, plan; index)`` (src/backproject.jl:378-386) or
-    ``backproject(views, mumap, psfs, dy; interpmeth, mode)`` (src/backproject.jl:395-411)."""
+    """``backproject(views, plan; index)`` (src/backproject.jl:170-178) or
+    ``backproject(views, mumap, psfs, dy; interpmeth, mode)`` (src/backproject.jl:187-203)."""
     if isinstance(plan_or_mumap, SPECTplan):
         plan = plan_or_mumap
     else:

@@ -8,7 +8,7 @@
 //                slices staged in shared memory.
 //   k_conv_fwd2  (conv2.cuh) depth-dependent PSF convolution and depth sum.
 //   k_reduce_views  sum of the chunk partials in chunk order (+ fused EM ratio).
-// Adjoint pass (backproject!, src/backproject.jl:277-332):
+// Adjoint pass (backproject!, src/backproject.jl:69-124):
 //   k_vspec2, k_conv_adj2 (conv2.cuh) adjoint PSF convolution -> T[slot][y][z][x].
 //   k_rot_adj    attenuation weighting and the exact transpose of the
 //                bilinear rotation (imrotate_adj! :two, src/rotatez.jl:390-416),
@@ -325,7 +325,7 @@ __host__ __device__ constexpr int acc_floats(int rows, int as) { return ((rows +
 // global per-CTA buffer) and adds/writes it into imgpart[split][z][:][:].
 // CACHED: a_s from the attenuation cache; otherwise rotated mu-map + depth
 // scan per view (imrotate! of the mu-map and the attenuation of
-// src/backproject.jl:285-317).
+// src/backproject.jl:77-109).
 constexpr int kRotAdjThreads = 512;
 
 template <bool CACHED>
