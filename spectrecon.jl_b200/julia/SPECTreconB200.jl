@@ -13,11 +13,20 @@
 #     views = project(image, plan)                 # host arrays, synchronous
 #     backproject!(image, views, plan; index = 1:2:plan.nview)
 #     xhat = osem(x0, ynoisy, background, Ablock(plan, 8); niter = 4)
+#
+# Ablock(plan, nblocks) returns the reference's Vector{LinearMapAO} (one
+# LinearMapAA per subset, src/ml-os-em.jl:70-84), so reference-style code that
+# indexes Ab[nb] and applies Ab[nb] * x, Ab[nb]' * y runs unchanged; osem!/mlem!
+# recognise maps built here from one plan and run the whole reconstruction as
+# one device-resident call, and fall back to the reference's loop otherwise.
 
 module SPECTreconB200
 
+using LinearAlgebra: mul!
+using LinearMapsAA: LinearMapAO, LinearMapAA
+
 export SPECTplan, project, project!, backproject, backproject!
-export mlem, mlem!, osem, osem!, Ablock, psf_gauss, autotune!, conv_kernels
+export mlem, mlem!, osem, osem!, Ablock, SPECTmap, psf_gauss, autotune!, conv_kernels
 
 const LIB = get(ENV, "SPECT_B200_LIB", joinpath(@__DIR__, "..", "libspectgpu.so"))
 
@@ -81,6 +90,10 @@ end
 
 _index(index) = Cint.(collect(index) .- 1) # 1-based Julia views -> 0-based C
 
+# the caller's array itself when it already is a dense Float32 Array (no copy)
+_f32(a::Array{Float32}) = a
+_f32(a::AbstractArray) = Array{Float32}(a)
+
 """
     project!(views, image, plan; index = 1:plan.nview)   (src/project.jl:143-163)
 """
@@ -91,11 +104,12 @@ function project!(
     index::AbstractVector{<:Int} = 1:plan.nview,
 )
     idx = _index(index)
-    out = Array{Float32}(undef, plan.imgsize[1], plan.imgsize[3], length(idx))
+    size(views) == (plan.imgsize[1], plan.imgsize[3], length(idx)) || throw(DimensionMismatch("views size"))
+    out = views isa Array{Float32, 3} ? views : Array{Float32}(undef, size(views))
     check(ccall((:spect_project_host, LIB), Cint,
         (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Ptr{Cint}, Cint),
-        plan.handle, out, Array{Float32}(image), idx, length(idx)))
-    views .= out
+        plan.handle, out, _f32(image), idx, length(idx)))
+    out === views || (views .= out)
     return views
 end
 
@@ -137,11 +151,12 @@ function backproject!(
     index::AbstractVector{<:Int} = 1:plan.nview,
 )
     idx = _index(index)
-    out = Array{Float32}(undef, plan.imgsize)
+    size(image) == plan.imgsize || throw(DimensionMismatch("image size"))
+    out = image isa Array{Float32, 3} ? image : Array{Float32}(undef, plan.imgsize)
     check(ccall((:spect_backproject_host, LIB), Cint,
         (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Ptr{Cint}, Cint),
-        plan.handle, out, Array{Float32}(views), idx, length(idx)))
-    image .= out
+        plan.handle, out, _f32(views), idx, length(idx)))
+    out === image || (image .= out)
     return image
 end
 
@@ -168,45 +183,117 @@ function backproject(views::AbstractArray{<:Real, 3}, mumap::AbstractArray{<:Rea
 end
 
 """
-    Ablock(plan, nblocks)  (src/ml-os-em.jl:70-84): the subsets nb:nblocks:nview
+    SPECTmap(plan; index = 1:plan.nview) -> LinearMapAO
+The projector of `plan` for the views `index` as a LinearMapAA (the map that
+test/adjoint-project.jl:33-35 builds from project!/backproject!), tagged with
+the plan so that mlem!/osem! can run it as one device-resident call.
 """
-struct Ablock
-    plan::SPECTplan
-    nblocks::Int
-    function Ablock(plan::SPECTplan, nblocks::Int)
-        rem(plan.nview, nblocks) == 0 || throw("nview must be divisible by nblocks!")
-        new(plan, nblocks)
-    end
+function SPECTmap(plan::SPECTplan; index::AbstractVector{<:Int} = 1:plan.nview, nblocks::Int = 1, block::Int = 1)
+    nx, ny, nz = plan.imgsize
+    forw!(y, x) = project!(y, x, plan; index)
+    back!(x, y) = backproject!(x, y, plan; index)
+    idim = (nx, ny, nz)
+    odim = (nx, nz, length(index))
+    return LinearMapAA(forw!, back!, (prod(odim), prod(idim)); T = plan.T, odim, idim,
+        prop = (plan = plan, nblocks = nblocks, block = block))
 end
-Base.length(Ab::Ablock) = Ab.nblocks
 
-function _em!(out, x0, ynoisy, background, plan::SPECTplan, nblocks::Int, niter::Int)
+"""
+    Ablock(plan, nblocks) -> Vector{LinearMapAO}  (src/ml-os-em.jl:70-84)
+One map per subset nb:nblocks:nview, as the reference returns.
+"""
+function Ablock(plan::SPECTplan, nblocks::Int)
+    rem(plan.nview, nblocks) == 0 || throw("nview must be divisible by nblocks!")
+    Ab = Vector{LinearMapAO}(undef, nblocks)
+    for nb in 1:nblocks
+        Ab[nb] = SPECTmap(plan; index = nb:nblocks:plan.nview, nblocks, block = nb)
+    end
+    return Ab
+end
+
+# the plan behind maps built by SPECTmap/Ablock from one plan covering all
+# views in the reference's subset order, or nothing
+_tagged(A) = A isa LinearMapAO && haskey(A.prop, :plan) ? A.prop : nothing
+function _plan_of(Ab::AbstractVector)
+    props = map(_tagged, Ab)
+    any(isnothing, props) && return nothing
+    plan = props[1].plan
+    n = length(Ab)
+    all(k -> props[k].plan === plan && props[k].nblocks == n && props[k].block == k, 1:n) || return nothing
+    return plan
+end
+
+function _em_checks(out, x0, ynoisy, background)
     all(>(0), background) || throw("need background > 0")
     size(out) == size(x0) || throw(DimensionMismatch("size out and x0 not match"))
     size(ynoisy) == size(background) || throw(DimensionMismatch("size ynoisy and background"))
-    res = Array{Float32}(undef, plan.imgsize)
+end
+
+# the whole OS-EM (nblocks = 1: ML-EM) as one call: sensitivities, iterations
+# and the fused EM ratio/update on the device
+function _em!(out, x0, ynoisy, background, plan::SPECTplan, nblocks::Int, niter::Int)
+    res = out isa Array{Float32, 3} && out !== x0 ? out : Array{Float32}(undef, plan.imgsize)
     check(ccall((:spect_osem_host, LIB), Cint,
         (Ptr{Cvoid}, Ptr{Float32}, Ptr{Float32}, Ptr{Float32}, Ptr{Float32}, Cint, Cint),
-        plan.handle, res, Array{Float32}(x0), Array{Float32}(ynoisy), Array{Float32}(background),
-        nblocks, niter))
-    out .= res
+        plan.handle, res, _f32(x0), _f32(ynoisy), _f32(background), nblocks, niter))
+    res === out || (out .= res)
+    return out
+end
+
+# the reference's OS-EM loop (src/ml-os-em.jl:106-131) for any maps
+function _em_generic!(out, x0, ynoisy, background, Ab, niter, chat)
+    nblocks = length(Ab)
+    nx, nz, nview = size(ynoisy)
+    asum = [Ab[nb]' * ones(eltype(ynoisy), nx, nz, nview ÷ nblocks) for nb in 1:nblocks]
+    for a in asum
+        a[a .== 0] .= Inf
+    end
+    ybar = Array{eltype(ynoisy)}(undef, nx, nz, nview ÷ nblocks)
+    yratio = similar(ybar)
+    back = similar(x0)
+    copyto!(out, x0)
+    for iter in 1:niter, nb in 1:nblocks
+        chat && (@show iter, nb, extrema(out))
+        mul!(ybar, Ab[nb], out)
+        @. yratio = (@view ynoisy[:, :, nb:nblocks:nview]) / (ybar + (@view background[:, :, nb:nblocks:nview]))
+        mul!(back, Ab[nb]', yratio)
+        @. out *= back / asum[nb]
+    end
     return out
 end
 
 """
-    mlem!(out, x0, ynoisy, background, plan; niter = 20)  (src/ml-os-em.jl:21-49)
-The system matrix is the plan itself (the reference takes the LinearMapAA that wraps it).
+    mlem!(out, x0, ynoisy, background, A; niter = 20)  (src/ml-os-em.jl:21-49)
+`A` as in the reference (AbstractArray or LinearMapAO); a map from SPECTmap
+(or the plan itself) runs as one device-resident call.
 """
-mlem!(out, x0, ynoisy, background, A::SPECTplan; niter::Int = 20, chat::Bool = false) =
-    _em!(out, x0, ynoisy, background, A, 1, niter)
-mlem(x0, args...; kwargs...) = mlem!(similar(x0, Float32), x0, args...; kwargs...)
+function mlem!(out::AbstractArray, x0::AbstractArray, ynoisy::AbstractArray, background::AbstractArray,
+    A::Union{AbstractArray, LinearMapAO}; niter::Int = 20, chat::Bool = false)
+    _em_checks(out, x0, ynoisy, background)
+    plan = _plan_of([A])
+    plan === nothing || return _em!(out, x0, ynoisy, background, plan, 1, niter)
+    return _em_generic!(out, x0, ynoisy, background, [A], niter, chat)
+end
+function mlem!(out::AbstractArray, x0::AbstractArray, ynoisy::AbstractArray, background::AbstractArray,
+    A::SPECTplan; niter::Int = 20, chat::Bool = false)
+    _em_checks(out, x0, ynoisy, background)
+    return _em!(out, x0, ynoisy, background, A, 1, niter)
+end
+mlem(x0::AbstractArray, args...; kwargs...) = mlem!(similar(x0, Float32), x0, args...; kwargs...)
 
 """
     osem!(out, x0, ynoisy, background, Ab; niter = 16)  (src/ml-os-em.jl:97-131)
+`Ab` as in the reference (a vector of arrays or LinearMapAOs); the maps of
+Ablock(plan, nblocks) run as one device-resident call.
 """
-osem!(out, x0, ynoisy, background, Ab::Ablock; niter::Int = 16, chat::Bool = false) =
-    _em!(out, x0, ynoisy, background, Ab.plan, Ab.nblocks, niter)
-osem(x0, args...; kwargs...) = osem!(similar(x0, Float32), x0, args...; kwargs...)
+function osem!(out::AbstractArray, x0::AbstractArray, ynoisy::AbstractArray, background::AbstractArray,
+    Ab::Union{Vector{<:AbstractArray}, Vector{LinearMapAO}}; niter::Int = 16, chat::Bool = false)
+    _em_checks(out, x0, ynoisy, background)
+    plan = _plan_of(Ab)
+    plan === nothing || return _em!(out, x0, ynoisy, background, plan, length(Ab), niter)
+    return _em_generic!(out, x0, ynoisy, background, Ab, niter, chat)
+end
+osem(x0::AbstractArray, args...; kwargs...) = osem!(similar(x0, Float32), x0, args...; kwargs...)
 
 """
     psf_gauss(; ny, px, pz, fwhm_start, fwhm_end, fwhm, fwhm_x, fwhm_z, T)  (src/psf-gauss.jl:24-55)
