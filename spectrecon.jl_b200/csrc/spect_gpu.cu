@@ -999,7 +999,7 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
     std::vector<int> fsh, ash;
     for (int i = 0; i < kZNShapes; ++i) {
       const int cap = kZShapes[i].nt * kZShapes[i].nth;
-      if (cap >= xtasks && cap <= 2 * xtasks && kZShapes[i].nth <= 640) fsh.push_back(i);
+      if (cap >= xtasks && cap <= 2 * xtasks && zfwd_shape_ok(i)) fsh.push_back(i);
       if (kZShapes[i].nt == 1 && kZShapes[i].nth <= 640) ash.push_back(i);
     }
     if (fsh.empty()) fsh.push_back(p->zshape_fwd);
@@ -1329,7 +1329,7 @@ int zpick_fwd(const ZGeom& g) {
   int best = -1;
   for (int i = 0; i < kZNShapes; ++i) {
     const int cap = kZShapes[i].nt * kZShapes[i].nth;
-    if (cap < xtasks || kZShapes[i].nth > 640) continue;  // 1024 threads leave too few registers
+    if (cap < xtasks || !zfwd_shape_ok(i)) continue;
     if (best < 0 || cap < kZShapes[best].nt * kZShapes[best].nth ||
         (cap == kZShapes[best].nt * kZShapes[best].nth && kZShapes[i].nth > kZShapes[best].nth))
       best = i;

@@ -57,11 +57,9 @@ namespace spect {
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
-// 8 taps of one 8-output task: o[k] += w[s] e[s + k], e = (p, q, r, t) the 16
-// consecutive window elements starting at the block's first tap
-__device__ __forceinline__ void zfma8(const float* __restrict__ w, float4 p, float4 q, float4 r, float4 t,
-                                      float (&o)[8]) {
-  const float4 w0 = ld4(w), w1 = ld4(w + 4);
+// 8 taps of one 8-output task: o[k] += ws[s] e[s + k], e = (p, q, r, t) the
+// 16 consecutive window elements starting at the block's first tap
+__device__ __forceinline__ void zfma8(float4 w0, float4 w1, float4 p, float4 q, float4 r, float4 t, float (&o)[8]) {
   const float ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
   const float e[16] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w, r.x, r.y, r.z, r.w, t.x, t.y, t.z, t.w};
 #pragma unroll
@@ -72,21 +70,46 @@ __device__ __forceinline__ void zfma8(const float* __restrict__ w, float4 p, flo
 
 // one 8-output task over a zero-padded line, the window in nblk blocks of 8
 // taps (nblk <= 9): o[k] += sum_{m < 8 nblk} w[m] line[k + m] (line and w
-// 16-byte aligned; reads line[0, 8 nblk + 8)).  Fully unrolled with a uniform
-// early exit: the window registers alternate by name, with no loop counter
-// or register moves.
+// 16-byte aligned; reads line[0, 8 nblk + 8)).  Unrolled with a uniform early
+// exit; the window's float4 quads rotate through three register pairs, and
+// each block's new pair is loaded one block ahead (shared-memory latency then
+// hides behind the previous block's 64 FMAs).  PF = false loads each pair
+// just before its block (fewer live registers, for register-bound callers).
+template <bool PF = true>
 __device__ __forceinline__ void zpassu(const float* __restrict__ w, int nblk, const float* line, float (&o)[8]) {
-  float4 a = ld4(line), b = ld4(line + 4), c, d;
+  float4 a = ld4(line), b = ld4(line + 4), c = ld4(line + 8), d = ld4(line + 12), e, f;
 #pragma unroll
-  for (int k = 0; k < 10; k += 2) {
+  for (int k = 0; k < 9; k += 3) {
     if (k >= nblk) break;
-    c = ld4(line + 8 * k + 8);
-    d = ld4(line + 8 * k + 12);
-    zfma8(w + 8 * k, a, b, c, d, o);
+    if (PF && k + 1 < nblk) {  // quads of block k + 1
+      e = ld4(line + 8 * k + 16);
+      f = ld4(line + 8 * k + 20);
+    }
+    zfma8(ld4(w + 8 * k), ld4(w + 8 * k + 4), a, b, c, d, o);
     if (k + 1 >= nblk) break;
-    a = ld4(line + 8 * k + 16);
-    b = ld4(line + 8 * k + 20);
-    zfma8(w + 8 * k + 8, c, d, a, b, o);
+    if (!PF) {
+      e = ld4(line + 8 * k + 16);
+      f = ld4(line + 8 * k + 20);
+    }
+    if (PF && k + 2 < nblk) {
+      a = ld4(line + 8 * k + 24);
+      b = ld4(line + 8 * k + 28);
+    }
+    zfma8(ld4(w + 8 * k + 8), ld4(w + 8 * k + 12), c, d, e, f, o);
+    if (k + 2 >= nblk) break;
+    if (!PF) {
+      a = ld4(line + 8 * k + 24);
+      b = ld4(line + 8 * k + 28);
+    }
+    if (PF && k + 3 < nblk) {
+      c = ld4(line + 8 * k + 32);
+      d = ld4(line + 8 * k + 36);
+    }
+    zfma8(ld4(w + 8 * k + 16), ld4(w + 8 * k + 20), e, f, a, b, o);
+    if (!PF && k + 3 < nblk) {
+      c = ld4(line + 8 * k + 32);
+      d = ld4(line + 8 * k + 36);
+    }
   }
 }
 
@@ -299,19 +322,38 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         }
         return;
       }
-      // rotated, attenuated plane into ZB (column x, rows R0 + z), four z at a time
-      for (int u = tid; u < units; u += NTH) {
-        const int x = zdiv(u, rnz4), zg = u - x * nz4;
-        const float4 w = geoW[x];
-        const float* p = a.img + geoO[x] + 4 * zg;
-        const float4 t0 = ld4(p), t1 = ld4(p + nzp), t2 = ld4(p + Lz), t3 = ld4(p + Lz + nzp);
-        const float4 at = ld4(sA + (size_t)x * nzp + 4 * zg);
-        float4 o;
-        o.x = __fmul_rn(fmaf(w.w, t3.x, fmaf(w.z, t2.x, fmaf(w.y, t1.x, __fmul_rn(w.x, t0.x)))), at.x);
-        o.y = __fmul_rn(fmaf(w.w, t3.y, fmaf(w.z, t2.y, fmaf(w.y, t1.y, __fmul_rn(w.x, t0.y)))), at.y);
-        o.z = __fmul_rn(fmaf(w.w, t3.z, fmaf(w.z, t2.z, fmaf(w.y, t1.z, __fmul_rn(w.x, t0.z)))), at.z);
-        o.w = __fmul_rn(fmaf(w.w, t3.w, fmaf(w.z, t2.w, fmaf(w.y, t1.w, __fmul_rn(w.x, t0.w)))), at.w);
-        st4(ZB + x * ast + R0 + 4 * zg, o);
+      // rotated, attenuated plane into ZB (column x, rows R0 + z), four z at a
+      // time, UB units a round with all their loads issued first (two when
+      // the x-pass accumulators leave the registers for it)
+      {
+        constexpr int UB = NT * NTH <= 1280 ? 2 : 1;
+        for (int u0 = tid; u0 < units; u0 += UB * NTH) {
+          int xs[UB], gs[UB];
+          float4 t[UB][4], at[UB], w[UB];
+#pragma unroll
+          for (int j = 0; j < UB; ++j) {
+            const int u = min(u0 + j * NTH, units - 1);  // a repeat of the last unit stores the same values
+            xs[j] = zdiv(u, rnz4);
+            gs[j] = u - xs[j] * nz4;
+            const float* pj = a.img + geoO[xs[j]] + 4 * gs[j];
+            t[j][0] = ld4(pj);
+            t[j][1] = ld4(pj + nzp);
+            t[j][2] = ld4(pj + Lz);
+            t[j][3] = ld4(pj + Lz + nzp);
+            w[j] = geoW[xs[j]];
+            at[j] = ld4(sA + xs[j] * nzp + 4 * gs[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < UB; ++j) {
+            const float4 wj = w[j], A = t[j][0], B = t[j][1], C = t[j][2], D = t[j][3], T4 = at[j];
+            float4 o;
+            o.x = __fmul_rn(fmaf(wj.w, D.x, fmaf(wj.z, C.x, fmaf(wj.y, B.x, __fmul_rn(wj.x, A.x)))), T4.x);
+            o.y = __fmul_rn(fmaf(wj.w, D.y, fmaf(wj.z, C.y, fmaf(wj.y, B.y, __fmul_rn(wj.x, A.y)))), T4.y);
+            o.z = __fmul_rn(fmaf(wj.w, D.z, fmaf(wj.z, C.z, fmaf(wj.y, B.z, __fmul_rn(wj.x, A.z)))), T4.z);
+            o.w = __fmul_rn(fmaf(wj.w, D.w, fmaf(wj.z, C.w, fmaf(wj.y, B.w, __fmul_rn(wj.x, A.w)))), T4.w);
+            st4(ZB + xs[j] * ast + R0 + 4 * gs[j], o);
+          }
+        }
       }
       __syncthreads();
       if (tid == 0) {  // next plane of this block into the staging buffers
@@ -357,7 +399,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         if (t < xtasks) {
           const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
           const float* row = XB + z * bs;
-          zpassu(Hw + zpw, xblk, row + x0, acc[i]);
+          zpassu<(NT <= 2)>(Hw + zpw, xblk, row + x0, acc[i]);
           if (x0 < hx) {
             const float e0 = row[C0];
 #pragma unroll
@@ -393,10 +435,10 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
 
 // ------------------------------------------------------------------------
 // k_zadj<NT, NTH>: adjoint convolution; work items (slot, depth chunk); the
-// view is loaded zero-padded once per item; per plane the adjoint weights
-// and folds are bulk-copied two planes deep; x pass (view rows) -> WB, z pass
-// (WB columns) -> times the attenuation column (global loads issued before
-// the pass) -> T.  NT only sets how the x tasks are interleaved.
+// view is loaded zero-padded once per item; per plane the attenuation plane,
+// adjoint weights and folds are bulk-copied two planes deep; x pass (view
+// rows) -> WB, z pass (WB columns) -> times the attenuation -> T.  NT only
+// sets how the x tasks are interleaved.
 template <int NT, int NTH>
 __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   extern __shared__ float4 smem4[];
@@ -404,18 +446,22 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts;
   float* const base = reinterpret_cast<float*>(smem4);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);  // two barriers
+  const int sts = nx * nzp + hs + ts;      // one stage: attenuation plane, weights, folds
   float* const stage = base + 4;
-  float* const VB = stage + 2 * (hs + ts);
+  float* const VB = stage + 2 * sts;
   float* const WB = VB + (size_t)nz * g.bs;
   const int tid = threadIdx.x;
   const int nitems = a.nv * a.nchunks;
   auto issue = [&](int item, int y, int b) {  // one thread
     const int sl = item / a.nchunks, v = a.vidx[sl], set = a.viewset[v];
-    float* st = stage + b * (hs + ts);
+    float* st = stage + b * sts;
+    const unsigned abytes = (unsigned)((size_t)nx * nzp * sizeof(float));
     fence_proxy_async();
-    mbar_expect(&bar[b], (unsigned)((hs + ts) * sizeof(float)));
-    bulk_copy(&bar[b], st, a.H + ((size_t)set * ny + y) * (2 * hs) + hs, (unsigned)(hs * sizeof(float)));
-    bulk_copy(&bar[b], st + hs, a.E + ((size_t)set * ny + y) * (2 * ts) + ts, (unsigned)(ts * sizeof(float)));
+    mbar_expect(&bar[b], abytes + (unsigned)((hs + ts) * sizeof(float)));
+    bulk_copy(&bar[b], st, a.att + ((size_t)v * ny + y) * nx * nzp, abytes);
+    bulk_copy(&bar[b], st + nx * nzp, a.H + ((size_t)set * ny + y) * (2 * hs) + hs, (unsigned)(hs * sizeof(float)));
+    bulk_copy(&bar[b], st + nx * nzp + hs, a.E + ((size_t)set * ny + y) * (2 * ts) + ts,
+              (unsigned)(ts * sizeof(float)));
   };
   auto next = [&](int& item, int& y) {
     const int yend = min(ny, (item % a.nchunks) * a.chunkY + a.chunkY);
@@ -472,7 +518,8 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
         return;
       }
       phases ^= 1u << b;
-      const float* st = stage + b * (hs + ts);
+      const float* sA = stage + b * sts;  // attenuation plane [x][nzp]
+      const float* st = sA + nx * nzp;
       const float* az = st;             // adjoint z weights (shifted)
       const float* ax = st + g.zpw;     // adjoint x weights (shifted)
       const float* cLx = st + hs;       // folds
@@ -499,11 +546,10 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
         }
       __syncthreads();
       // z pass: task (x, z block) -> T column (x, y) of the slot
-      const float* attv = a.att + (((size_t)v * ny + y) * nx) * nzp;
       float* Tp = a.T + (((size_t)slot * ny + y) * nx) * nzp;
       for (int t = tid; t < ztasks; t += NTH) {
         const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = 8 * zb;
-        const float4 a0 = ld4(attv + x * nzp + z0), a1 = ld4(attv + x * nzp + z0 + 4);
+        const float4 a0 = ld4(sA + x * nzp + z0), a1 = ld4(sA + x * nzp + z0 + 4);
         const float* col = WB + x * ast;
         float o[8];
 #pragma unroll
@@ -569,31 +615,38 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
       const int xlo = max(0, (int)ceilf(xc - rr)), xhi = min(nx - 1, (int)floorf(xc + rr));
       const int ylo = max(0, (int)ceilf(yc - rr)), yhi = min(ny - 1, (int)floorf(yc + rr));
       const float* Ts = T + (size_t)s * ny * nx * nzp + lane;
+      // the candidates first (weights, column offsets; 0 for the invalid
+      // ones), then their loads, so that a group has all of them in flight
+      float cw[9];
+      int co[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
-        const int xx = xlo + i;
-        if (xx > xhi) break;
+        const int xx = min(xlo + i, nx - 1);
         const float di = __fsub_rn((float)xx, c0);
         const float ca = __fmul_rn(cs, di), cc = __fmul_rn(sn, di);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          const int yy = ylo + k;
-          if (yy > yhi) break;
+          const int yy = min(ylo + k, ny - 1);
           const float dj = __fsub_rn((float)yy, c0);
           const float s1 = __fadd_rn(c0, __fsub_rn(ca, __fmul_rn(sn, dj)));
           const float s2 = __fadd_rn(c0, __fadd_rn(cc, __fmul_rn(cs, dj)));
-          if (s1 >= fj1 - 1.f && s1 < fj1 + 1.f && s2 >= fj2 - 1.f && s2 < fj2 + 1.f) {
-            const float f1 = floorf(s1), f2 = floorf(s2);
-            const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
-            const float a1 = f1 == fj1 ? __fsub_rn(1.0f, t1) : t1;
-            const float a2 = f2 == fj2 ? __fsub_rn(1.0f, t2) : t2;
-            const float w = __fmul_rn(a1, a2);
-            const float* tp = Ts + ((size_t)yy * nx + xx) * nzp;
-#pragma unroll
-            for (int q = 0; q < ZPL; ++q) acc[q] = fmaf(w, tp[8 * q], acc[q]);
-          }
+          const bool ok = xlo + i <= xhi && ylo + k <= yhi && s1 >= fj1 - 1.f && s1 < fj1 + 1.f &&
+                          s2 >= fj2 - 1.f && s2 < fj2 + 1.f;
+          const float f1 = floorf(s1), f2 = floorf(s2);
+          const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
+          const float a1 = f1 == fj1 ? __fsub_rn(1.0f, t1) : t1;
+          const float a2 = f2 == fj2 ? __fsub_rn(1.0f, t2) : t2;
+          cw[3 * i + k] = ok ? __fmul_rn(a1, a2) : 0.f;
+          co[3 * i + k] = ok ? (yy * nx + xx) * nzp : -1;
         }
       }
+#pragma unroll
+      for (int c = 0; c < 9; ++c)
+        if (co[c] >= 0) {
+          const float* tp = Ts + co[c];
+#pragma unroll
+          for (int q = 0; q < ZPL; ++q) acc[q] = fmaf(cw[c], tp[8 * q], acc[q]);
+        }
     }
     const size_t o = ((size_t)(j2 + g.pad) * g.L + j1 + g.pad) * nzp + lane;
 #pragma unroll

@@ -77,11 +77,11 @@ __host__ __device__ inline size_t zfwd_smem(const ZGeom& g) {
   return f * sizeof(float);
 }
 
-// k_zadj shared memory (floats): [bar 4][2 stages x (hs + ts)]
-//   [VB nz * bs: the view, zero-padded, data columns C0..][WB nx * ast:
-//   x-pass output, column x, data rows R0..]
+// k_zadj shared memory (floats): [bar 4][2 stages x (attenuation plane
+//   nx*nzp | weights hs | folds ts)][VB nz * bs: the view, zero-padded, data
+//   columns C0..][WB nx * ast: x-pass output, column x, data rows R0..]
 __host__ __device__ inline size_t zadj_smem(const ZGeom& g) {
-  return sizeof(float) * (4 + 2 * (size_t)(g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)g.nx * g.ast);
+  return sizeof(float) * (4 + 2 * ((size_t)g.nx * g.nzp + g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)g.nx * g.ast);
 }
 
 // launch shapes of k_zfwd / k_zadj: NT tasks per thread, NTH threads
@@ -90,6 +90,9 @@ struct ZShape {
 };
 constexpr int kZNShapes = 8;
 constexpr ZShape kZShapes[kZNShapes] = {{1, 512}, {2, 512}, {3, 512}, {4, 512}, {1, 640}, {2, 640}, {3, 640}, {1, 1024}};
+// forward shapes that compile without register spills: not 3 x 640 and not
+// 1024 threads (their accumulators leave too few registers)
+inline bool zfwd_shape_ok(int i) { return !(kZShapes[i].nt == 3 && kZShapes[i].nth == 640) && kZShapes[i].nth <= 640; }
 
 // launchers (zpath_inst.cu)
 cudaError_t zpath_setup(int max_smem);
