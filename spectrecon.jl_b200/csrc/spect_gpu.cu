@@ -235,6 +235,10 @@ struct spect_plan_s {
   float* d_Hz = nullptr;       // [nset][ny][2 hs] pass weights
   float* d_Ez = nullptr;       // [nset][ny][2 ts] forward tails, adjoint folds
   int zshape_fwd = -1, zshape_adj = -1;
+  // split kernels with the gather rotation adjoint: the premultiplied adjoint
+  // planes are transposed into d_Tz (z fastest) and gathered into d_backIZ
+  int gadj = 0;
+  float* d_Tz = nullptr;
   size_t zfwd_smem_b = 0, zadj_smem_b = 0;
   size_t bytes = 0;
   // stream on which the plan is built and its buffers are (de)allocated;
@@ -265,7 +269,7 @@ void free_plan(spect_plan_s* p) {
   void* ptrs[] = {p->d_mumap, p->d_att, p->d_err, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
-                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep, p->d_imgIZ, p->d_backIZ, p->d_Hz, p->d_Ez};
+                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep, p->d_imgIZ, p->d_backIZ, p->d_Hz, p->d_Ez, p->d_Tz};
   for (void* q : ptrs)
     if (q) {
       if (p->async_alloc) cudaFreeAsync(q, p->home);
@@ -733,7 +737,13 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     }
     dim3 grid(g.nz, nsplit);
     const size_t rsm = p->rota_smem_ok ? p->rota_smem : 0;
-    if (p->interp == SPECT_INTERP_ONE) {
+    if (p->gadj) {  // premultiplied planes -> z fastest -> gather into the IZ accumulator
+      LAUNCH(p, K_ROT_ADJ, st, "k_t_to_z", zt_to_z_launch(p->zg, nv * g.ny, st, p->d_P, p->d_Tz));
+      const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 8, 256));
+      LAUNCH(p, K_ROT_ADJ, st, "k_zrot_adj",
+             zrot_adj_launch(p->zg, grot, st, p->d_Tz, p->d_rot, vi, nv, g0 > 0 ? p->d_backIZ : nullptr, p->d_backIZ,
+                             nullptr, nullptr, 0));
+    } else if (p->interp == SPECT_INTERP_ONE) {
       const size_t n = (size_t)nv * p->N;
       LAUNCH(p, K_ROT_ADJ, st, "k_att_combine",
              k_att_combine<true><<<(int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16), 256, 0, st>>>(
@@ -755,6 +765,11 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
            else k_rot_adj<false><<<grid, kRotAdjThreads, rsm, st>>>(
                g, p->d_P, p->d_mumap, p->d_att, p->d_rot, vi, nv, p->d_imgpart, g0 > 0 ? 1 : 0, p->rota_smem_ok,
                p->d_gscr_adj));
+  }
+  if (p->gadj) {
+    if (nidx == 0) CUDA_TRY(cudaMemsetAsync(p->d_backIZ, 0, sizeof(float) * p->izN, st));
+    LAUNCH(p, K_REDUCE_IMAGE, st, "k_from_iz", zfrom_iz_launch(p->zg, st, p->d_backIZ, image, asum, mode));
+    return SPECT_OK;
   }
   int rb = (int)std::min<size_t>((p->N + 255) / 256, (size_t)p->sm_count * 16);
   LAUNCH(p, K_REDUCE_IMAGE, st, "k_reduce_image",
@@ -1507,6 +1522,21 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       (st = dalloc(p, &p->d_Vs, (size_t)p->gmax * p->cg.Q * Npx)) ||
       (st = dalloc(p, &p->d_imgpart, (size_t)p->nsplit_adj_max * p->N)))
     return bail(st);
+  {  // split kernels whose adjoint planes come premultiplied (attenuation cache,
+     // :two): rotation adjoint by the gather kernel (SPECT_GADJ=0 keeps the
+     // scatter kernels)
+    const char* genv = std::getenv("SPECT_GADJ");
+    if (!p->zpath && p->adj_stage && interpmeth == SPECT_INTERP_TWO && zg.nzp <= 256 && !(genv && genv[0] == '0')) {
+      p->gadj = 1;
+      p->zg = zg;
+      p->izN = (size_t)zg.L * zg.L * zg.nzp;
+      if ((st = dalloc(p, &p->d_backIZ, p->izN)) ||
+          (st = dalloc(p, &p->d_Tz, (size_t)p->gmax * ny * nx * zg.nzp)))
+        return bail(st);
+      if (cudaMemsetAsync(p->d_backIZ, 0, sizeof(float) * p->izN, p->home) != cudaSuccess)
+        return bail(fail(SPECT_ERR_CUDA, "memset"));
+    }
+  }
   if (p->zpath) {  // IZ volumes (zero ring and z padding) and zeroed adjoint planes
     if ((st = dalloc(p, &p->d_imgIZ, p->izN)) || (st = dalloc(p, &p->d_backIZ, p->izN)))
       return bail(st);
@@ -2236,6 +2266,7 @@ size_t est_job_bytes(const ServerJob& j, bool att) {
              + 8 * N + 2 * (size_t)j.nview * nxz + (size_t)j.nblocks * N  // imgpart, EM buffers
              + 2 * N + 2 * (size_t)j.nview * nxz;     // job buffers
   if (j.interp == SPECT_INTERP_ONE) f += nsub * N;
+  else f += nsub * (size_t)j.nx * j.nx * ((j.nz + 15) / 16 * 16) + 2 * N;  // z-fastest planes, IZ volumes
   size_t b = 4 * f + (size_t)j.nview * 32;
   // per-CTA global slabs of large planes (B, spectra accumulators)
   if ((size_t)j.nx * (Q + 1) * 8 + 8192 > 227 * 1024) b += (size_t)148 * j.nx * (Q + 1) * 8;

@@ -162,6 +162,27 @@ __global__ void __launch_bounds__(256) k_from_iz(ZGeom g, const float* __restric
   }
 }
 
+// k_t_to_z: adjoint planes of the split kernels ([plane][nz][nx], plane =
+// slot * ny + y) into the z-fastest T layout ([plane][nx][nzp], zeros for
+// z >= nz) that k_zrot_adj reads; grid (ceil(nx/32), planes, ceil(nzp/32)),
+// block (32, 8).
+__global__ void __launch_bounds__(256) k_t_to_z(ZGeom g, const float* __restrict__ src, float* __restrict__ dst) {
+  __shared__ float tile[32][33];
+  const int x0 = blockIdx.x * 32, pl = blockIdx.y, z0 = blockIdx.z * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const float* s = src + (size_t)pl * g.nz * g.nx;
+  float* d = dst + (size_t)pl * g.nx * g.nzp;
+  for (int k = ty; k < 32; k += 8) {  // tile[z][x], coalesced over x
+    const int z = z0 + k, x = x0 + tx;
+    tile[k][tx] = (z < g.nz && x < g.nx) ? s[(size_t)z * g.nx + x] : 0.f;
+  }
+  __syncthreads();
+  for (int k = ty; k < 32; k += 8) {  // column x, coalesced over z
+    const int x = x0 + k, z = z0 + tx;
+    if (x < g.nx && z < g.nzp) d[(size_t)x * g.nzp + z] = tile[tx][k];
+  }
+}
+
 // ------------------------------------------------------------------------
 // Geometry of rotated-grid point (x, y) of a view, with the forward
 // sampling's products and sums in the same order and rounding

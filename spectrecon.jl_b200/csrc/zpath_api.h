@@ -102,6 +102,7 @@ cudaError_t zrot_adj_launch(const ZGeom& g, int grid, cudaStream_t st, const flo
                             const int* vidx, int nv, const float* prev, float* out, const float* x, const float* asum,
                             int mode);
 cudaError_t zto_iz_launch(const ZGeom& g, cudaStream_t st, const float* img, float* iz);
+cudaError_t zt_to_z_launch(const ZGeom& g, int planes, cudaStream_t st, const float* src, float* dst);
 cudaError_t zfrom_iz_launch(const ZGeom& g, cudaStream_t st, const float* iz, float* dst, const float* asum, int mode);
 cudaError_t zatten_launch(const ZGeom& g, int nview, cudaStream_t st, const float* muz, const float4* rot, float dy,
                           float* att);

@@ -59,6 +59,11 @@ cudaError_t zto_iz_launch(const ZGeom& g, cudaStream_t st, const float* img, flo
   return cudaGetLastError();
 }
 
+cudaError_t zt_to_z_launch(const ZGeom& g, int planes, cudaStream_t st, const float* src, float* dst) {
+  k_t_to_z<<<dim3((g.nx + 31) / 32, planes, (g.nzp + 31) / 32), dim3(32, 8), 0, st>>>(g, src, dst);
+  return cudaGetLastError();
+}
+
 cudaError_t zfrom_iz_launch(const ZGeom& g, cudaStream_t st, const float* iz, float* dst, const float* asum, int mode) {
   k_from_iz<<<dim3((g.nx + 31) / 32, g.ny, (g.nz + 31) / 32), dim3(32, 8), 0, st>>>(g, iz, dst, asum, mode);
   return cudaGetLastError();
