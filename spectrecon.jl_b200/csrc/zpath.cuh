@@ -71,44 +71,50 @@ __device__ __forceinline__ void zfma8(float4 w0, float4 w1, float4 p, float4 q, 
 // one 8-output task over a zero-padded line, the window in nblk blocks of 8
 // taps (nblk <= 9): o[k] += sum_{m < 8 nblk} w[m] line[k + m] (line and w
 // 16-byte aligned; reads line[0, 8 nblk + 8)).  Unrolled with a uniform early
-// exit; the window's float4 quads rotate through three register pairs, and
-// each block's new pair is loaded one block ahead (shared-memory latency then
-// hides behind the previous block's 64 FMAs).  PF = false loads each pair
-// just before its block (fewer live registers, for register-bound callers).
+// exit; the window's float4 quads rotate through three register pairs and the
+// weights through two; with PF each block's new quads and weights are loaded
+// one block ahead, so shared-memory latency hides behind the previous block's
+// 64 FMAs (PF = false loads them just before their block, with fewer live
+// registers, for register-bound callers).
 template <bool PF = true>
 __device__ __forceinline__ void zpassu(const float* __restrict__ w, int nblk, const float* line, float (&o)[8]) {
   float4 a = ld4(line), b = ld4(line + 4), c = ld4(line + 8), d = ld4(line + 12), e, f;
+  float4 w0 = ld4(w), w1 = ld4(w + 4), w2, w3;
 #pragma unroll
-  for (int k = 0; k < 9; k += 3) {
+  for (int k = 0; k < 9; k += 2) {
+    // blocks k (quads by k mod 3) and k + 1; weights (w0, w1) for even, (w2, w3) for odd blocks
     if (k >= nblk) break;
-    if (PF && k + 1 < nblk) {  // quads of block k + 1
-      e = ld4(line + 8 * k + 16);
-      f = ld4(line + 8 * k + 20);
+    const int r = k % 3;  // rotation phase of block k
+    float4 &p0 = r == 0 ? a : r == 1 ? c : e, &p1 = r == 0 ? b : r == 1 ? d : f;
+    float4 &p2 = r == 0 ? c : r == 1 ? e : a, &p3 = r == 0 ? d : r == 1 ? f : b;
+    float4 &n0 = r == 0 ? e : r == 1 ? a : c, &n1 = r == 0 ? f : r == 1 ? b : d;
+    if (PF && k + 1 < nblk) {  // quads and weights of block k + 1
+      n0 = ld4(line + 8 * k + 16);
+      n1 = ld4(line + 8 * k + 20);
+      w2 = ld4(w + 8 * k + 8);
+      w3 = ld4(w + 8 * k + 12);
     }
-    zfma8(ld4(w + 8 * k), ld4(w + 8 * k + 4), a, b, c, d, o);
+    zfma8(w0, w1, p0, p1, p2, p3, o);
     if (k + 1 >= nblk) break;
     if (!PF) {
-      e = ld4(line + 8 * k + 16);
-      f = ld4(line + 8 * k + 20);
+      n0 = ld4(line + 8 * k + 16);
+      n1 = ld4(line + 8 * k + 20);
+      w2 = ld4(w + 8 * k + 8);
+      w3 = ld4(w + 8 * k + 12);
     }
+    // block k + 1 uses (p2, p3, n0, n1); its successor needs the pair after n1
     if (PF && k + 2 < nblk) {
-      a = ld4(line + 8 * k + 24);
-      b = ld4(line + 8 * k + 28);
+      p0 = ld4(line + 8 * k + 24);
+      p1 = ld4(line + 8 * k + 28);
+      w0 = ld4(w + 8 * k + 16);
+      w1 = ld4(w + 8 * k + 20);
     }
-    zfma8(ld4(w + 8 * k + 8), ld4(w + 8 * k + 12), c, d, e, f, o);
-    if (k + 2 >= nblk) break;
-    if (!PF) {
-      a = ld4(line + 8 * k + 24);
-      b = ld4(line + 8 * k + 28);
-    }
-    if (PF && k + 3 < nblk) {
-      c = ld4(line + 8 * k + 32);
-      d = ld4(line + 8 * k + 36);
-    }
-    zfma8(ld4(w + 8 * k + 16), ld4(w + 8 * k + 20), e, f, a, b, o);
-    if (!PF && k + 3 < nblk) {
-      c = ld4(line + 8 * k + 32);
-      d = ld4(line + 8 * k + 36);
+    zfma8(w2, w3, p2, p3, n0, n1, o);
+    if (!PF && k + 2 < nblk) {
+      p0 = ld4(line + 8 * k + 24);
+      p1 = ld4(line + 8 * k + 28);
+      w0 = ld4(w + 8 * k + 16);
+      w1 = ld4(w + 8 * k + 20);
     }
   }
 }
@@ -390,7 +396,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) o[k] = 0.f;
         const float* col = ZB + x * ast;
-        zpassu(Hw, zblk, col + z0, o);
+        zpassu<(NT <= 2)>(Hw, zblk, col + z0, o);
         if (z0 < hz) {  // clamped rows above the plane
           const float e0 = col[R0];
 #pragma unroll
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         if (t < xtasks) {
           const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
           const float* row = XB + z * bs;
-          zpassu<(NT <= 2)>(Hw + zpw, xblk, row + x0, acc[i]);
+          zpassu<(NT <= 1)>(Hw + zpw, xblk, row + x0, acc[i]);
           if (x0 < hx) {
             const float e0 = row[C0];
 #pragma unroll
@@ -456,10 +462,10 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
 
 // ------------------------------------------------------------------------
 // k_zadj<NT, NTH>: adjoint convolution; work items (slot, depth chunk); the
-// view is loaded zero-padded once per item; per plane the attenuation plane,
-// adjoint weights and folds are bulk-copied two planes deep; x pass (view
-// rows) -> WB, z pass (WB columns) -> times the attenuation -> T.  NT only
-// sets how the x tasks are interleaved.
+// view is loaded zero-padded once per item; per plane the adjoint weights and
+// folds are bulk-copied two planes deep; x pass (view rows) -> WB, z pass (WB
+// columns) -> times the attenuation column (16-byte global loads issued at
+// the task's start) -> T.  NT only sets how the x tasks are interleaved.
 template <int NT, int NTH>
 __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   extern __shared__ float4 smem4[];
@@ -467,7 +473,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts;
   float* const base = reinterpret_cast<float*>(smem4);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);  // two barriers
-  const int sts = nx * nzp + hs + ts;      // one stage: attenuation plane, weights, folds
+  const int sts = hs + ts;                 // one stage: weights, folds
   float* const stage = base + 4;
   float* const VB = stage + 2 * sts;
   float* const WB = VB + (size_t)nz * g.bs;
@@ -476,13 +482,10 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   auto issue = [&](int item, int y, int b) {  // one thread
     const int sl = item / a.nchunks, v = a.vidx[sl], set = a.viewset[v];
     float* st = stage + b * sts;
-    const unsigned abytes = (unsigned)((size_t)nx * nzp * sizeof(float));
     fence_proxy_async();
-    mbar_expect(&bar[b], abytes + (unsigned)((hs + ts) * sizeof(float)));
-    bulk_copy(&bar[b], st, a.att + ((size_t)v * ny + y) * nx * nzp, abytes);
-    bulk_copy(&bar[b], st + nx * nzp, a.H + ((size_t)set * ny + y) * (2 * hs) + hs, (unsigned)(hs * sizeof(float)));
-    bulk_copy(&bar[b], st + nx * nzp + hs, a.E + ((size_t)set * ny + y) * (2 * ts) + ts,
-              (unsigned)(ts * sizeof(float)));
+    mbar_expect(&bar[b], (unsigned)((hs + ts) * sizeof(float)));
+    bulk_copy(&bar[b], st, a.H + ((size_t)set * ny + y) * (2 * hs) + hs, (unsigned)(hs * sizeof(float)));
+    bulk_copy(&bar[b], st + hs, a.E + ((size_t)set * ny + y) * (2 * ts) + ts, (unsigned)(ts * sizeof(float)));
   };
   auto next = [&](int& item, int& y) {
     const int yend = min(ny, (item % a.nchunks) * a.chunkY + a.chunkY);
@@ -539,8 +542,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
         return;
       }
       phases ^= 1u << b;
-      const float* sA = stage + b * sts;  // attenuation plane [x][nzp]
-      const float* st = sA + nx * nzp;
+      const float* st = stage + b * sts;
       const float* az = st;             // adjoint z weights (shifted)
       const float* ax = st + g.zpw;     // adjoint x weights (shifted)
       const float* cLx = st + hs;       // folds
@@ -567,10 +569,11 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
         }
       __syncthreads();
       // z pass: task (x, z block) -> T column (x, y) of the slot
+      const float* attv = a.att + (((size_t)v * ny + y) * nx) * nzp;
       float* Tp = a.T + (((size_t)slot * ny + y) * nx) * nzp;
       for (int t = tid; t < ztasks; t += NTH) {
         const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = 8 * zb;
-        const float4 a0 = ld4(sA + x * nzp + z0), a1 = ld4(sA + x * nzp + z0 + 4);
+        const float4 a0 = ld4(attv + x * nzp + z0), a1 = ld4(attv + x * nzp + z0 + 4);
         const float* col = WB + x * ast;
         float o[8];
 #pragma unroll

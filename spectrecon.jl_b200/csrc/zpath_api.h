@@ -77,11 +77,11 @@ __host__ __device__ inline size_t zfwd_smem(const ZGeom& g) {
   return f * sizeof(float);
 }
 
-// k_zadj shared memory (floats): [bar 4][2 stages x (attenuation plane
-//   nx*nzp | weights hs | folds ts)][VB nz * bs: the view, zero-padded, data
-//   columns C0..][WB nx * ast: x-pass output, column x, data rows R0..]
+// k_zadj shared memory (floats): [bar 4][2 stages x (weights hs | folds ts)]
+//   [VB nz * bs: the view, zero-padded, data columns C0..][WB nx * ast:
+//   x-pass output, column x, data rows R0..]
 __host__ __device__ inline size_t zadj_smem(const ZGeom& g) {
-  return sizeof(float) * (4 + 2 * ((size_t)g.nx * g.nzp + g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)g.nx * g.ast);
+  return sizeof(float) * (4 + 2 * (size_t)(g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)g.nx * g.ast);
 }
 
 // launch shapes of k_zfwd / k_zadj: NT tasks per thread, NTH threads
