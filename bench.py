@@ -727,6 +727,32 @@ def oracle_recon(st, dtype=np.float32, nthread=None):
     return out, time.perf_counter() - t0
 
 
+def oracle_calibration():
+    """The oracle on the reference's own timing case (time/project.jl:16-31:
+    project! of a 64x64x40 image, 60 views, random symmetric 19x19 PSFs,
+    :two, all threads), best of 3, beside the reference's published time for
+    that call (289.8 ms, time/project.jl:60-61, on the reference authors'
+    machine)."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(0)
+    nx, nz, nview, p = 64, 40, 60, 19
+    mumap = np.asfortranarray(rng.random((nx, nx, nz)), np.float32)
+    psfs = rng.random((p, p, nx, nview))
+    psfs = psfs + psfs[::-1, ::-1]
+    psfs = psfs + psfs.transpose(1, 0, 2, 3)
+    psfs = np.asfortranarray(psfs / psfs.sum(axis=(0, 1), keepdims=True), np.float32)
+    G = O.Geometry(mumap, psfs, 4.7952)
+    x = np.asfortranarray(rng.random((nx, nx, nz)), np.float32)
+    best = 1e30
+    for _ in range(3):
+        t0 = time.perf_counter()
+        G.project(x)
+        best = min(best, time.perf_counter() - t0)
+    return {"case": "project! 64x64x40, 60 views, 19x19 PSF, :two (time/project.jl)",
+            "oracle_ms": round(1e3 * best, 1), "cores": os.cpu_count(), "reference_published_ms": 289.8}
+
+
 def cpu_baseline(st, gpu_out=None):
     """The oracle on the host cores: one full Float32 OS-EM reconstruction of
     the benchmark study, measured (not extrapolated).  With ``gpu_out`` (the
@@ -737,7 +763,7 @@ def cpu_baseline(st, gpu_out=None):
     res = {"value": round(1.0 / t32, 6), "unit": "recons/s", "cores": os.cpu_count(), "kind": "port",
            "sample": f"one full OS-EM reconstruction of the same study ({st.nblocks} subsets x {st.niter} "
                      f"iterations, {st.nview} views), Float32, measured",
-           "sample_seconds": round(t32, 2)}
+           "sample_seconds": round(t32, 2), "calibration": oracle_calibration()}
     parity = None
     if gpu_out is not None:
         out64, t64 = oracle_recon(st, np.float64)
@@ -785,7 +811,8 @@ def run_reference(args):
            "data": "synthetic (seeded phantoms)", "config": dict(CONFIG),
            "path": "CPU oracle: restatement of the reference's threaded project!/backproject!/osem! (no Julia)",
            "cpu_baseline": {"value": round(v, 6), "unit": "recons/s", "cores": os.cpu_count(), "kind": "port",
-                            "sample": "every step one full OS-EM reconstruction of the study, measured"},
+                            "sample": "every step one full OS-EM reconstruction of the study, measured",
+                            "calibration": oracle_calibration()},
            "e2e": {"value": round(v, 6), "unit": "recons/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
            "wall_s": round(wall, 1)}
     print(json.dumps(res), flush=True)
