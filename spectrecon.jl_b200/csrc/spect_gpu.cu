@@ -738,7 +738,8 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     dim3 grid(g.nz, nsplit);
     const size_t rsm = p->rota_smem_ok ? p->rota_smem : 0;
     if (p->gadj) {  // premultiplied planes -> z fastest -> gather into the IZ accumulator
-      LAUNCH(p, K_ROT_ADJ, st, "k_t_to_z", zt_to_z_launch(p->zg, nv * g.ny, st, p->d_P, p->d_Tz));
+      LAUNCH(p, K_ROT_ADJ, st, "k_t_to_z",
+             zt_to_z_launch(p->zg, nv * g.ny, st, p->d_P, p->d_Tz, p->adj_stage ? nullptr : p->d_att, vi));
       const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 8, 256));
       LAUNCH(p, K_ROT_ADJ, st, "k_zrot_adj",
              zrot_adj_launch(p->zg, grot, st, p->d_Tz, p->d_rot, vi, nv, g0 > 0 ? p->d_backIZ : nullptr, p->d_backIZ,
@@ -1522,11 +1523,11 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       (st = dalloc(p, &p->d_Vs, (size_t)p->gmax * p->cg.Q * Npx)) ||
       (st = dalloc(p, &p->d_imgpart, (size_t)p->nsplit_adj_max * p->N)))
     return bail(st);
-  {  // split kernels whose adjoint planes come premultiplied (attenuation cache,
-     // :two): rotation adjoint by the gather kernel (SPECT_GADJ=0 keeps the
-     // scatter kernels)
+  {  // split kernels with the attenuation cache (:two): rotation adjoint by the
+     // gather kernel, the attenuation applied by the convolution's store or by
+     // the transpose (SPECT_GADJ=0 keeps the scatter kernels)
     const char* genv = std::getenv("SPECT_GADJ");
-    if (!p->zpath && p->adj_stage && interpmeth == SPECT_INTERP_TWO && zg.nzp <= 256 && !(genv && genv[0] == '0')) {
+    if (!p->zpath && p->d_att && interpmeth == SPECT_INTERP_TWO && zg.nzp <= 256 && !(genv && genv[0] == '0')) {
       p->gadj = 1;
       p->zg = zg;
       p->izN = (size_t)zg.L * zg.L * zg.nzp;

@@ -57,9 +57,11 @@ namespace spect {
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
-// 8 taps of one 8-output task: o[k] += ws[s] e[s + k], e = (p, q, r, t) the
-// 16 consecutive window elements starting at the block's first tap
-__device__ __forceinline__ void zfma8(float4 w0, float4 w1, float4 p, float4 q, float4 r, float4 t, float (&o)[8]) {
+// 8 taps of one 8-output task: o[k] += w[s] e[s + k], e = (p, q, r, t) the 16
+// consecutive window elements starting at the block's first tap
+__device__ __forceinline__ void zfma8(const float* __restrict__ w, float4 p, float4 q, float4 r, float4 t,
+                                      float (&o)[8]) {
+  const float4 w0 = ld4(w), w1 = ld4(w + 4);
   const float ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
   const float e[16] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w, r.x, r.y, r.z, r.w, t.x, t.y, t.z, t.w};
 #pragma unroll
@@ -70,52 +72,23 @@ __device__ __forceinline__ void zfma8(float4 w0, float4 w1, float4 p, float4 q, 
 
 // one 8-output task over a zero-padded line, the window in nblk blocks of 8
 // taps (nblk <= 9): o[k] += sum_{m < 8 nblk} w[m] line[k + m] (line and w
-// 16-byte aligned; reads line[0, 8 nblk + 8)).  Unrolled with a uniform early
-// exit; the window's float4 quads rotate through three register pairs and the
-// weights through two; with PF each block's new quads and weights are loaded
-// one block ahead, so shared-memory latency hides behind the previous block's
-// 64 FMAs (PF = false loads them just before their block, with fewer live
-// registers, for register-bound callers).
-template <bool PF = true>
+// 16-byte aligned; reads line[0, 8 nblk + 8)).  Fully unrolled with a uniform
+// early exit: the window registers alternate by name, with no loop counter or
+// register moves.  (Loading the next block's quads and weights a block ahead
+// was measured slower on the benchmark study: more instructions and shared
+// queue pressure for less latency.)
 __device__ __forceinline__ void zpassu(const float* __restrict__ w, int nblk, const float* line, float (&o)[8]) {
-  float4 a = ld4(line), b = ld4(line + 4), c = ld4(line + 8), d = ld4(line + 12), e, f;
-  float4 w0 = ld4(w), w1 = ld4(w + 4), w2, w3;
+  float4 a = ld4(line), b = ld4(line + 4), c, d;
 #pragma unroll
-  for (int k = 0; k < 9; k += 2) {
-    // blocks k (quads by k mod 3) and k + 1; weights (w0, w1) for even, (w2, w3) for odd blocks
+  for (int k = 0; k < 10; k += 2) {
     if (k >= nblk) break;
-    const int r = k % 3;  // rotation phase of block k
-    float4 &p0 = r == 0 ? a : r == 1 ? c : e, &p1 = r == 0 ? b : r == 1 ? d : f;
-    float4 &p2 = r == 0 ? c : r == 1 ? e : a, &p3 = r == 0 ? d : r == 1 ? f : b;
-    float4 &n0 = r == 0 ? e : r == 1 ? a : c, &n1 = r == 0 ? f : r == 1 ? b : d;
-    if (PF && k + 1 < nblk) {  // quads and weights of block k + 1
-      n0 = ld4(line + 8 * k + 16);
-      n1 = ld4(line + 8 * k + 20);
-      w2 = ld4(w + 8 * k + 8);
-      w3 = ld4(w + 8 * k + 12);
-    }
-    zfma8(w0, w1, p0, p1, p2, p3, o);
+    c = ld4(line + 8 * k + 8);
+    d = ld4(line + 8 * k + 12);
+    zfma8(w + 8 * k, a, b, c, d, o);
     if (k + 1 >= nblk) break;
-    if (!PF) {
-      n0 = ld4(line + 8 * k + 16);
-      n1 = ld4(line + 8 * k + 20);
-      w2 = ld4(w + 8 * k + 8);
-      w3 = ld4(w + 8 * k + 12);
-    }
-    // block k + 1 uses (p2, p3, n0, n1); its successor needs the pair after n1
-    if (PF && k + 2 < nblk) {
-      p0 = ld4(line + 8 * k + 24);
-      p1 = ld4(line + 8 * k + 28);
-      w0 = ld4(w + 8 * k + 16);
-      w1 = ld4(w + 8 * k + 20);
-    }
-    zfma8(w2, w3, p2, p3, n0, n1, o);
-    if (!PF && k + 2 < nblk) {
-      p0 = ld4(line + 8 * k + 24);
-      p1 = ld4(line + 8 * k + 28);
-      w0 = ld4(w + 8 * k + 16);
-      w1 = ld4(w + 8 * k + 20);
-    }
+    a = ld4(line + 8 * k + 16);
+    b = ld4(line + 8 * k + 20);
+    zfma8(w + 8 * k + 8, c, d, a, b, o);
   }
 }
 
@@ -170,17 +143,23 @@ __global__ void __launch_bounds__(256) k_from_iz(ZGeom g, const float* __restric
 
 // k_t_to_z: adjoint planes of the split kernels ([plane][nz][nx], plane =
 // slot * ny + y) into the z-fastest T layout ([plane][nx][nzp], zeros for
-// z >= nz) that k_zrot_adj reads; grid (ceil(nx/32), planes, ceil(nzp/32)),
+// z >= nz) that k_zrot_adj reads, multiplied by the attenuation when the
+// convolution has not applied it (att non-null, the same product as the
+// reference's a_y .* conv_adj); grid (ceil(nx/32), planes, ceil(nzp/32)),
 // block (32, 8).
-__global__ void __launch_bounds__(256) k_t_to_z(ZGeom g, const float* __restrict__ src, float* __restrict__ dst) {
+__global__ void __launch_bounds__(256) k_t_to_z(ZGeom g, const float* __restrict__ src, float* __restrict__ dst,
+                                                const float* __restrict__ att, const int* __restrict__ vidx) {
   __shared__ float tile[32][33];
   const int x0 = blockIdx.x * 32, pl = blockIdx.y, z0 = blockIdx.z * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const float* s = src + (size_t)pl * g.nz * g.nx;
   float* d = dst + (size_t)pl * g.nx * g.nzp;
+  // att (split layout [view][y][z][x]) given: the planes are not premultiplied yet
+  const float* av = att ? att + ((size_t)vidx[pl / g.ny] * g.ny + pl % g.ny) * g.nz * g.nx : nullptr;
   for (int k = ty; k < 32; k += 8) {  // tile[z][x], coalesced over x
     const int z = z0 + k, x = x0 + tx;
-    tile[k][tx] = (z < g.nz && x < g.nx) ? s[(size_t)z * g.nx + x] : 0.f;
+    const size_t o = (size_t)z * g.nx + x;
+    tile[k][tx] = (z < g.nz && x < g.nx) ? (av ? __fmul_rn(av[o], s[o]) : s[o]) : 0.f;
   }
   __syncthreads();
   for (int k = ty; k < 32; k += 8) {  // column x, coalesced over z
@@ -349,38 +328,19 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         }
         return;
       }
-      // rotated, attenuated plane into ZB (column x, rows R0 + z), four z at a
-      // time, UB units a round with all their loads issued first (two when
-      // the x-pass accumulators leave the registers for it)
-      {
-        constexpr int UB = NT * NTH <= 1280 ? 2 : 1;
-        for (int u0 = tid; u0 < units; u0 += UB * NTH) {
-          int xs[UB], gs[UB];
-          float4 t[UB][4], at[UB], w[UB];
-#pragma unroll
-          for (int j = 0; j < UB; ++j) {
-            const int u = min(u0 + j * NTH, units - 1);  // a repeat of the last unit stores the same values
-            xs[j] = zdiv(u, rnz4);
-            gs[j] = u - xs[j] * nz4;
-            const float* pj = a.img + geoO[xs[j]] + 4 * gs[j];
-            t[j][0] = ld4(pj);
-            t[j][1] = ld4(pj + nzp);
-            t[j][2] = ld4(pj + Lz);
-            t[j][3] = ld4(pj + Lz + nzp);
-            w[j] = geoW[xs[j]];
-            at[j] = ld4(sA + xs[j] * nzp + 4 * gs[j]);
-          }
-#pragma unroll
-          for (int j = 0; j < UB; ++j) {
-            const float4 wj = w[j], A = t[j][0], B = t[j][1], C = t[j][2], D = t[j][3], T4 = at[j];
-            float4 o;
-            o.x = __fmul_rn(fmaf(wj.w, D.x, fmaf(wj.z, C.x, fmaf(wj.y, B.x, __fmul_rn(wj.x, A.x)))), T4.x);
-            o.y = __fmul_rn(fmaf(wj.w, D.y, fmaf(wj.z, C.y, fmaf(wj.y, B.y, __fmul_rn(wj.x, A.y)))), T4.y);
-            o.z = __fmul_rn(fmaf(wj.w, D.z, fmaf(wj.z, C.z, fmaf(wj.y, B.z, __fmul_rn(wj.x, A.z)))), T4.z);
-            o.w = __fmul_rn(fmaf(wj.w, D.w, fmaf(wj.z, C.w, fmaf(wj.y, B.w, __fmul_rn(wj.x, A.w)))), T4.w);
-            st4(ZB + xs[j] * ast + R0 + 4 * gs[j], o);
-          }
-        }
+      // rotated, attenuated plane into ZB (column x, rows R0 + z), four z at a time
+      for (int u = tid; u < units; u += NTH) {
+        const int x = zdiv(u, rnz4), zg = u - x * nz4;
+        const float4 w = geoW[x];
+        const float* p = a.img + geoO[x] + 4 * zg;
+        const float4 t0 = ld4(p), t1 = ld4(p + nzp), t2 = ld4(p + Lz), t3 = ld4(p + Lz + nzp);
+        const float4 at = ld4(sA + x * nzp + 4 * zg);
+        float4 o;
+        o.x = __fmul_rn(fmaf(w.w, t3.x, fmaf(w.z, t2.x, fmaf(w.y, t1.x, __fmul_rn(w.x, t0.x)))), at.x);
+        o.y = __fmul_rn(fmaf(w.w, t3.y, fmaf(w.z, t2.y, fmaf(w.y, t1.y, __fmul_rn(w.x, t0.y)))), at.y);
+        o.z = __fmul_rn(fmaf(w.w, t3.z, fmaf(w.z, t2.z, fmaf(w.y, t1.z, __fmul_rn(w.x, t0.z)))), at.z);
+        o.w = __fmul_rn(fmaf(w.w, t3.w, fmaf(w.z, t2.w, fmaf(w.y, t1.w, __fmul_rn(w.x, t0.w)))), at.w);
+        st4(ZB + x * ast + R0 + 4 * zg, o);
       }
       __syncthreads();
       if (tid == 0) {  // next plane of this block into the staging buffers
@@ -396,7 +356,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) o[k] = 0.f;
         const float* col = ZB + x * ast;
-        zpassu<(NT <= 2)>(Hw, zblk, col + z0, o);
+        zpassu(Hw, zblk, col + z0, o);
         if (z0 < hz) {  // clamped rows above the plane
           const float e0 = col[R0];
 #pragma unroll
@@ -426,7 +386,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         if (t < xtasks) {
           const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
           const float* row = XB + z * bs;
-          zpassu<(NT <= 1)>(Hw + zpw, xblk, row + x0, acc[i]);
+          zpassu(Hw + zpw, xblk, row + x0, acc[i]);
           if (x0 < hx) {
             const float e0 = row[C0];
 #pragma unroll

@@ -90,9 +90,9 @@ struct ZShape {
 };
 constexpr int kZNShapes = 8;
 constexpr ZShape kZShapes[kZNShapes] = {{1, 512}, {2, 512}, {3, 512}, {4, 512}, {1, 640}, {2, 640}, {3, 640}, {1, 1024}};
-// forward shapes that compile without register spills: not 3 x 640 and not
-// 1024 threads (their accumulators leave too few registers)
-inline bool zfwd_shape_ok(int i) { return !(kZShapes[i].nt == 3 && kZShapes[i].nth == 640) && kZShapes[i].nth <= 640; }
+// forward shapes that compile without register spills: not 1024 threads
+// (with the accumulators they leave too few registers)
+inline bool zfwd_shape_ok(int i) { return kZShapes[i].nth <= 640; }
 
 // launchers (zpath_inst.cu)
 cudaError_t zpath_setup(int max_smem);
@@ -102,7 +102,8 @@ cudaError_t zrot_adj_launch(const ZGeom& g, int grid, cudaStream_t st, const flo
                             const int* vidx, int nv, const float* prev, float* out, const float* x, const float* asum,
                             int mode);
 cudaError_t zto_iz_launch(const ZGeom& g, cudaStream_t st, const float* img, float* iz);
-cudaError_t zt_to_z_launch(const ZGeom& g, int planes, cudaStream_t st, const float* src, float* dst);
+cudaError_t zt_to_z_launch(const ZGeom& g, int planes, cudaStream_t st, const float* src, float* dst,
+                            const float* att, const int* vidx);
 cudaError_t zfrom_iz_launch(const ZGeom& g, cudaStream_t st, const float* iz, float* dst, const float* asum, int mode);
 cudaError_t zatten_launch(const ZGeom& g, int nview, cudaStream_t st, const float* muz, const float4* rot, float dy,
                           float* att);

@@ -59,8 +59,9 @@ cudaError_t zto_iz_launch(const ZGeom& g, cudaStream_t st, const float* img, flo
   return cudaGetLastError();
 }
 
-cudaError_t zt_to_z_launch(const ZGeom& g, int planes, cudaStream_t st, const float* src, float* dst) {
-  k_t_to_z<<<dim3((g.nx + 31) / 32, planes, (g.nzp + 31) / 32), dim3(32, 8), 0, st>>>(g, src, dst);
+cudaError_t zt_to_z_launch(const ZGeom& g, int planes, cudaStream_t st, const float* src, float* dst,
+                            const float* att, const int* vidx) {
+  k_t_to_z<<<dim3((g.nx + 31) / 32, planes, (g.nzp + 31) / 32), dim3(32, 8), 0, st>>>(g, src, dst, att, vidx);
   return cudaGetLastError();
 }
 
