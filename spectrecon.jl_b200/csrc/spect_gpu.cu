@@ -585,7 +585,7 @@ int zbackward(spect_plan_s* p, float* outIZ, const float* views, const int* vidx
     CUDA_TRY(cudaMemsetAsync(outIZ, 0, sizeof(float) * p->izN, st));
     return SPECT_OK;
   }
-  const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 8, 256));  // 8 lanes per image column
+  const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 16, 256));  // 16 lanes per image column
   for (int g0 = 0; g0 < nidx; g0 += p->gmax) {
     const int nv = std::min(p->gmax, nidx - g0);
     const int* vi = vidx + g0;
@@ -740,7 +740,7 @@ int backward(spect_plan_s* p, float* image, const float* views, const int* vidx,
     if (p->gadj) {  // premultiplied planes -> z fastest -> gather into the IZ accumulator
       LAUNCH(p, K_ROT_ADJ, st, "k_t_to_z",
              zt_to_z_launch(p->zg, nv * g.ny, st, p->d_P, p->d_Tz, p->adj_stage ? nullptr : p->d_att, vi));
-      const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 8, 256));
+      const int grot = std::max(1, cdiv((long long)p->nx * p->nx * 16, 256));
       LAUNCH(p, K_ROT_ADJ, st, "k_zrot_adj",
              zrot_adj_launch(p->zg, grot, st, p->d_Tz, p->d_rot, vi, nv, g0 > 0 ? p->d_backIZ : nullptr, p->d_backIZ,
                              nullptr, nullptr, 0));

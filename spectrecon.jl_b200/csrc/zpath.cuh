@@ -564,15 +564,16 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 }
 
 // ------------------------------------------------------------------------
-// k_zrot_adj<ZPL>: an 8-lane group owns image column p = (j1, j2)
-// (grid-stride), lane l the z values l + 8 q, q < ZPL (nzp = 8 ZPL): one
-// 32-byte sector per lane group and load, and the candidate geometry shared
-// by the group's 8 lanes (4 columns per warp).  For every slot s in order,
-// the rotated-grid points (x, y) whose bilinear footprint contains (j1, j2)
-// -- those with floor(s1) in {j1-1, j1} and floor(s2) in {j2-1, j2} -- lie
-// within |cos| + |sin| of the inverse-rotated pixel centre, so the candidates
-// are at most 3 x 3 points; each is tested with the forward's own position
-// arithmetic and weighted with the forward's weight product.
+// k_zrot_adj<ZPL>: two 8-lane groups of a warp own image column p = (j1, j2)
+// (grid-stride), lane l of a group the z values l + 8 q, q < ZPL (nzp =
+// 8 ZPL): one 32-byte sector per group and load, the candidate geometry shared
+// by the group's 8 lanes.  The first group sums the even slots, the second
+// the odd ones; a shuffle adds the two partial sums (a fixed order).  For
+// every slot, the rotated-grid points (x, y) whose bilinear footprint contains
+// (j1, j2) -- those with floor(s1) in {j1-1, j1} and floor(s2) in {j2-1, j2}
+// -- lie within |cos| + |sin| of the inverse-rotated pixel centre, so the
+// candidates are at most 3 x 3 points; each is tested with the forward's own
+// position arithmetic and weighted with the forward's weight product.
 // Epilogue (IZ layout): v = acc (+ prev); mode 1: zeros -> +Inf; mode 2:
 // v = x * (v / asum); out = v (z < nz only; out may be prev or x).
 template <int ZPL>
@@ -580,17 +581,20 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
                                                  const float4* __restrict__ rot, const int* __restrict__ vidx, int nv,
                                                  const float* prev, float* out, const float* x,
                                                  const float* __restrict__ asum, int mode) {
-  const int lane = threadIdx.x & 7;
-  const int ngr = (gridDim.x * blockDim.x) >> 3;
+  const int lane = threadIdx.x & 7, half = (threadIdx.x >> 3) & 1;
+  const int npix = (gridDim.x * blockDim.x) >> 4;
   const int nx = g.nx, ny = g.ny, nzp = g.nzp;
   const float c0 = g.c0;
-  for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; p < nx * nx; p += ngr) {
+  // every warp runs the same number of iterations (the shuffle needs all lanes)
+  for (int p0 = (blockIdx.x * blockDim.x + (threadIdx.x & ~31)) >> 4; p0 < nx * nx; p0 += npix) {
+    const int p = min(p0 + ((threadIdx.x >> 4) & 1), nx * nx - 1);
+    const bool own = p0 + ((threadIdx.x >> 4) & 1) < nx * nx;
     const int j2 = p / nx, j1 = p - j2 * nx;
     const float fj1 = (float)j1, fj2 = (float)j2;
     float acc[ZPL];
 #pragma unroll
     for (int q = 0; q < ZPL; ++q) acc[q] = 0.f;
-    for (int s = 0; s < nv; ++s) {
+    for (int s = half; s < nv; s += 2) {
       const float4 r = rot[vidx[s]];
       const float cs = r.x, sn = r.y;
       const float d1 = fj1 - c0, d2 = fj2 - c0;
@@ -632,6 +636,9 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
           for (int q = 0; q < ZPL; ++q) acc[q] = fmaf(cw[c], tp[8 * q], acc[q]);
         }
     }
+#pragma unroll
+    for (int q = 0; q < ZPL; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], 8);  // even + odd slots
+    if (half || !own) continue;
     const size_t o = ((size_t)(j2 + g.pad) * g.L + j1 + g.pad) * nzp + lane;
 #pragma unroll
     for (int q = 0; q < ZPL; ++q) {
