@@ -128,7 +128,10 @@ int spect_project_host(spect_plan_t plan, float* views, const float* image, cons
  * stream capture.  All calls share the array and no part of it needs to
  * start at zero, but calls that overlap on the GPU (other streams, other
  * threads) race on it: serialise them.  Device pointers, enqueued on
- * stream; the plan's device must be the current device. */
+ * stream; the plan's device must be the current device.  The array's device
+ * address is looked up once per device and kept for the life of the process,
+ * so resetting a device (cudaDeviceReset) while the library is loaded is not
+ * supported by this entry point. */
 int spect_project_static_scratch(spect_plan_t plan, float* views, const float* image, const int32_t* index,
                                  int nindex, void* stream);
 
@@ -231,6 +234,22 @@ int spect_server_destroy(spect_server_t server);
  * index 0 k_rot_fwd, 1 k_conv_fwd, 2 k_reduce_views, 3 k_vspec,
  * 4 k_conv_adj, 5 k_rot_adj, 6 k_reduce_image, 7 other. */
 unsigned long long spect_kernel_launches(void);
+
+/* Failure detection of the bounded device waits (no counterpart in the
+ * reference).  Every kernel that waits for a bulk copy into shared memory
+ * polls its mbarrier a bounded number of times; on give-up it sets the plan's
+ * error flag and returns, so the context stays usable.  The *_host entry
+ * points report the flag as SPECT_ERR_TIMEOUT; callers of the asynchronous
+ * (device-pointer) entry points read and clear it with
+ * spect_plan_check_error(plan), which synchronises the plan's flag read on
+ * `stream` and returns SPECT_OK or SPECT_ERR_TIMEOUT.
+ * spect_selftest_wait_timeout() exercises the give-up path on the current
+ * device: one block waits a short bounded time on an mbarrier whose single
+ * expected arrival never happens, records the give-up and returns; the call returns
+ * SPECT_ERR_TIMEOUT when that path worked (and SPECT_ERR_CUDA if the kernel
+ * failed).  Synchronous; allocates 4 bytes. */
+int spect_plan_check_error(spect_plan_t plan, void* stream);
+int spect_selftest_wait_timeout(void);
 int spect_plan_profile(spect_plan_t plan, int on);
 int spect_plan_kernel_times(spect_plan_t plan, double ms[8], long long counts[8]);
 

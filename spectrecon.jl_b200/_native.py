@@ -58,6 +58,8 @@ _SIGS = {
     "spect_server_destroy": ([_P], _I),
     "spect_kernel_launches": ([], ctypes.c_ulonglong),
     "spect_fp32_peak": ([ctypes.POINTER(_D)], _I),
+    "spect_plan_check_error": ([_P, _P], _I),
+    "spect_selftest_wait_timeout": ([], _I),
     "spect_plan_profile": ([_P, _I], _I),
     "spect_plan_kernel_times": ([_P, _P, _P], _I),
     "spect_psf_gauss": ([_P, _I, _I, _I, _P, _P], _I),

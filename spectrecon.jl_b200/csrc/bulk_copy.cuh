@@ -32,8 +32,9 @@ __device__ __forceinline__ void tma_planes(unsigned long long* bar, float* dst0,
 }
 
 // bounded wait for the phase with the given parity; false when it gave up
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  for (int it = 0; it < (1 << 22); ++it) {
+// after `limit` polls
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, int limit = 1 << 22) {
+  for (int it = 0; it < limit; ++it) {
     unsigned ok;
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"

@@ -2094,6 +2094,20 @@ unsigned long long spect_kernel_launches(void) { return g_launches.load(); }
 }  // extern "C"
 
 namespace {
+// the give-up path of the bounded mbarrier wait: a barrier that expects one
+// arrival nobody makes (no copy is involved), a short bounded wait, the give-up
+// recorded as the projector kernels' error exit does, and a normal return
+__global__ void k_wait_giveup(int* err) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) mbar_init(&bar);
+  __syncthreads();
+  const bool ok = mbar_wait(&bar, 0u, 1 << 12);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+    return;
+  }
+}
+
 // independent FMA chains (x <- x a + b), 16 a thread: the FP32 pipe's rate
 __global__ void __launch_bounds__(512) k_fma_chains(float* out, int iters, float a, float b) {
   float x[16];
@@ -2110,6 +2124,37 @@ __global__ void __launch_bounds__(512) k_fma_chains(float* out, int iters, float
 }  // namespace
 
 extern "C" {
+
+int spect_plan_check_error(spect_plan_t p, void* stream) {
+  if (!p) return fail(SPECT_ERR_ARG, "null plan");
+  std::lock_guard<std::mutex> lk(p->mu);
+  int h = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (h) {
+    CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return fail(SPECT_ERR_TIMEOUT, "a bulk copy into shared memory did not complete");
+  }
+  return SPECT_OK;
+}
+
+int spect_selftest_wait_timeout(void) {
+  int* d = nullptr;
+  CUDA_TRY(cudaMalloc(&d, sizeof(int)));
+  cudaError_t e = cudaMemset(d, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    k_wait_giveup<<<1, 32>>>(d);
+    e = cudaGetLastError();
+  }
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(SPECT_ERR_CUDA, std::string("wait self-test: ") + cudaGetErrorString(e));
+  if (h == 1) return fail(SPECT_ERR_TIMEOUT, "bounded wait gave up as intended (self-test)");
+  return fail(SPECT_ERR_CUDA, "wait self-test: the bounded wait did not report its give-up");
+}
 
 int spect_fp32_peak(double* tflops) {
   if (!tflops) return fail(SPECT_ERR_ARG, "null pointer argument");

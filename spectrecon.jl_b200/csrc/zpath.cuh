@@ -57,11 +57,10 @@ namespace spect {
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
-// 8 taps of one 8-output task: o[k] += w[s] e[s + k], e = (p, q, r, t) the 16
-// consecutive window elements starting at the block's first tap
-__device__ __forceinline__ void zfma8(const float* __restrict__ w, float4 p, float4 q, float4 r, float4 t,
-                                      float (&o)[8]) {
-  const float4 w0 = ld4(w), w1 = ld4(w + 4);
+// 8 taps of one 8-output task: o[k] += w[s] e[s + k], with the block's
+// weights (w0, w1) and e = (p, q, r, t) the 16 consecutive window elements
+// starting at the block's first tap
+__device__ __forceinline__ void zfma8(float4 w0, float4 w1, float4 p, float4 q, float4 r, float4 t, float (&o)[8]) {
   const float ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
   const float e[16] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w, r.x, r.y, r.z, r.w, t.x, t.y, t.z, t.w};
 #pragma unroll
@@ -73,22 +72,40 @@ __device__ __forceinline__ void zfma8(const float* __restrict__ w, float4 p, flo
 // one 8-output task over a zero-padded line, the window in nblk blocks of 8
 // taps (nblk <= 9): o[k] += sum_{m < 8 nblk} w[m] line[k + m] (line and w
 // 16-byte aligned; reads line[0, 8 nblk + 8)).  Fully unrolled with a uniform
-// early exit: the window registers alternate by name, with no loop counter or
-// register moves.  (Loading the next block's quads and weights a block ahead
-// was measured slower on the benchmark study: more instructions and shared
-// queue pressure for less latency.)
+// early exit: the window quads alternate between two register pairs by name
+// (no loop counter or register moves), and the next block's weights are
+// loaded one block ahead, so a block's FMAs never start by waiting for them
+// (PF = false: loaded at the block, for callers short of registers).
+template <bool PF = true>
 __device__ __forceinline__ void zpassu(const float* __restrict__ w, int nblk, const float* line, float (&o)[8]) {
   float4 a = ld4(line), b = ld4(line + 4), c, d;
+  float4 wa0 = ld4(w), wa1 = ld4(w + 4), wb0, wb1;
 #pragma unroll
   for (int k = 0; k < 10; k += 2) {
     if (k >= nblk) break;
     c = ld4(line + 8 * k + 8);
     d = ld4(line + 8 * k + 12);
-    zfma8(w + 8 * k, a, b, c, d, o);
+    if (PF && k + 1 < nblk) {
+      wb0 = ld4(w + 8 * k + 8);
+      wb1 = ld4(w + 8 * k + 12);
+    }
+    if (!PF && k > 0) {
+      wa0 = ld4(w + 8 * k);
+      wa1 = ld4(w + 8 * k + 4);
+    }
+    zfma8(wa0, wa1, a, b, c, d, o);
     if (k + 1 >= nblk) break;
     a = ld4(line + 8 * k + 16);
     b = ld4(line + 8 * k + 20);
-    zfma8(w + 8 * k + 8, c, d, a, b, o);
+    if (PF && k + 2 < nblk) {
+      wa0 = ld4(w + 8 * k + 16);
+      wa1 = ld4(w + 8 * k + 20);
+    }
+    if (!PF) {
+      wb0 = ld4(w + 8 * k + 8);
+      wb1 = ld4(w + 8 * k + 12);
+    }
+    zfma8(wb0, wb1, c, d, a, b, o);
   }
 }
 
@@ -356,7 +373,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
 #pragma unroll
         for (int k = 0; k < 8; ++k) o[k] = 0.f;
         const float* col = ZB + x * ast;
-        zpassu(Hw, zblk, col + z0, o);
+        zpassu<(NT <= 2)>(Hw, zblk, col + z0, o);
         if (z0 < hz) {  // clamped rows above the plane
           const float e0 = col[R0];
 #pragma unroll
@@ -386,7 +403,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         if (t < xtasks) {
           const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
           const float* row = XB + z * bs;
-          zpassu(Hw + zpw, xblk, row + x0, acc[i]);
+          zpassu<(NT <= 2)>(Hw + zpw, xblk, row + x0, acc[i]);
           if (x0 < hx) {
             const float e0 = row[C0];
 #pragma unroll
