@@ -170,15 +170,19 @@ def launch_work(plan, kind, nv):
     of kernel kind `kind` processing nv views, for the path the plan runs.
     FLOPs count the convolution taps (1 FMA = 2 FLOP per tap of the z and x
     passes) plus the bilinear sample and attenuation; bytes count each
-    compulsory array once (attenuation planes, adjoint planes, images)."""
+    compulsory array once (attenuation planes, adjoint planes, images).  The
+    fused pair counts the taps it keeps per plane (the outer taps below
+    Float32 resolution of a plane's factors are skipped), so its fraction
+    measures the arithmetic it does, not the full-width work it avoids."""
     nx, ny, nz = plan.imgsize
     px, pz = plan.px, plan.pz
     N, nxz = nx * ny * nz, nx * nz
     nzp = 16 * ((nz + 15) // 16)
     if plan.fused:
+        tz, tx = plan.conv_taps()
         table = {
-            "k_conv_fwd": ("k_zfwd", "fp32", nv * ny * nx * nz * (2.0 * (px + pz) + 8), 4.0 * (nv * ny * nx * nzp + N)),
-            "k_conv_adj": ("k_zadj", "fp32", nv * ny * nx * nz * (2.0 * (px + pz) + 1), 4.0 * (2 * nv * ny * nx * nzp + nv * nxz)),
+            "k_conv_fwd": ("k_zfwd", "fp32", nv * ny * nx * nz * (2.0 * (tx + tz) + 8), 4.0 * (nv * ny * nx * nzp + N)),
+            "k_conv_adj": ("k_zadj", "fp32", nv * ny * nx * nz * (2.0 * (tx + tz) + 1), 4.0 * (2 * nv * ny * nx * nzp + nv * nxz)),
             "k_rot_adj": ("k_zrot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * ny * nx * nzp + 3 * N)),
             "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz),
             "k_reduce_image": ("k_from_iz", "hbm", 0.0, 4.0 * 2 * N),
@@ -371,7 +375,9 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantoms)",
         "config": dict(CONFIG),
         "path": ("fused projector pair" if plan.fused else "split kernels") + " (device-resident OS-EM), autotuned",
-        "convolution": {"forward": conv["forward"], "adjoint": conv["adjoint"]}, "parity": parity,
+        "convolution": {"forward": conv["forward"], "adjoint": conv["adjoint"],
+                        "taps_per_plane_z_x": [round(t, 2) for t in plan.conv_taps()], "psf_taps_z_x": [plan.pz, plan.px]},
+        "parity": parity,
         "e2e": {"value": round(e2e_value, 3), "unit": "recons/s",
                 "h2d_bytes_per_step": int(4 * (plan.imgsize[0] * ny * nz + 2 * nx * nz * nview)),
                 "d2h_bytes_per_step": int(4 * nx * ny * nz), "ms_per_step": round(e2e_ms / e2e_steps, 3),

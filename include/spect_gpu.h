@@ -104,6 +104,14 @@ int spect_plan_conv_kernels(spect_plan_t plan, int out[4]);
  * the reference (query of this implementation's kernel choice). */
 int spect_plan_fused(spect_plan_t plan, int* fused);
 
+/* taps[0], taps[1]: mean number of PSF taps per depth plane that the plan's
+ * z and x convolution passes run.  The fused pair skips the outer taps of
+ * each plane's factors whose summed magnitude per side is within 2^-27 of the
+ * factor's (below Float32 resolution; SPECT_ZTRIM=0 keeps them); other plans
+ * report pz and px.  No counterpart in the reference (work accounting of this
+ * implementation). */
+int spect_plan_fused_taps(spect_plan_t plan, double* taps);
+
 /* project!(views, image, plan; index) (src/project.jl:143-163).
  * views[nindex][nz][nx] = P_{index[i]} image; index NULL = all views in order
  * (nindex must then be nview).  Device pointers, enqueued on stream. */

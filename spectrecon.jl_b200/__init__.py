@@ -205,6 +205,14 @@ class SPECTplan:
         check(_native.lib().spect_plan_fused(self._h, ctypes.byref(out)))
         return bool(out.value)
 
+    def conv_taps(self):
+        """Mean PSF taps per depth plane that the z and x convolution passes
+        run: the fused pair skips the outer taps below Float32 resolution of
+        each plane's factors; other plans report (pz, px)."""
+        out = (ctypes.c_double * 2)()
+        check(_native.lib().spect_plan_fused_taps(self._h, out))
+        return float(out[0]), float(out[1])
+
     def autotune(self, nindex=None):
         """Time candidate launch shapes for calls with nindex views (default
         nview) and keep the fastest; returns (forward_ms, adjoint_ms)."""

@@ -35,6 +35,7 @@ _SIGS = {
     "spect_plan_info": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_Z)], _I),
     "spect_plan_conv_kernels": ([_P, ctypes.POINTER(_I)], _I),
     "spect_plan_fused": ([_P, ctypes.POINTER(_I)], _I),
+    "spect_plan_fused_taps": ([_P, ctypes.POINTER(ctypes.c_double)], _I),
     "spect_project": ([_P, _P, _P, _P, _I, _P], _I),
     "spect_project_host": ([_P, _P, _P, _P, _I], _I),
     "spect_project_static_scratch": ([_P, _P, _P, _P, _I, _P], _I),

@@ -234,6 +234,8 @@ struct spect_plan_s {
   float* d_backIZ = nullptr;   // back-projection accumulator (IZ)
   float* d_Hz = nullptr;       // [nset][ny][2 hs] pass weights
   float* d_Ez = nullptr;       // [nset][ny][2 ts] forward tails, adjoint folds
+  int* d_Rz = nullptr;         // [nset][ny][8] tap-block ranges of the four passes
+  double ztaps[2] = {0, 0};    // mean kept taps per plane of the fused passes (z, x)
   int zshape_fwd = -1, zshape_adj = -1;
   // split kernels with the gather rotation adjoint: the premultiplied adjoint
   // planes are transposed into d_Tz (z fastest) and gathered into d_backIZ
@@ -269,7 +271,7 @@ void free_plan(spect_plan_s* p) {
   void* ptrs[] = {p->d_mumap, p->d_att, p->d_err, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
-                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep, p->d_imgIZ, p->d_backIZ, p->d_Hz, p->d_Ez, p->d_Tz};
+                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep, p->d_imgIZ, p->d_backIZ, p->d_Hz, p->d_Ez, p->d_Tz, p->d_Rz};
   for (void* q : ptrs)
     if (q) {
       if (p->async_alloc) cudaFreeAsync(q, p->home);
@@ -543,6 +545,7 @@ ZArgs zargs(const spect_plan_s* p) {
   a.att = p->d_att;
   a.H = p->d_Hz;
   a.E = p->d_Ez;
+  a.R = p->d_Rz;
   a.rot = p->d_rot;
   a.viewset = p->d_viewset;
   a.err = p->d_err;
@@ -949,6 +952,8 @@ std::string tune_key(const spect_plan_s* p, int nv) {
          "/z" + std::to_string(p->zpath) + "/y" + std::to_string(p->ny);
 }
 
+bool zshape_allowed(const ZGeom& g, int i);
+
 int time_pass(spect_plan_s* p, bool adj, int nv, int reps, double* ms) {
   cudaStream_t st = p->home;
   cudaEvent_t a, b;
@@ -1011,10 +1016,10 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
   }
   if (p->zpath) {
     // fused path: depth tile and launch shape per direction
-    const int xtasks = p->nz * (p->nx / 8);
     std::vector<int> fsh, ash;
     for (int i = 0; i < kZNShapes; ++i) {
-      const int cap = kZShapes[i].nt * kZShapes[i].nth;
+      if (!zshape_allowed(p->zg, i)) continue;
+      const int cap = kZShapes[i].nt * kZShapes[i].nth, xtasks = p->nz * (p->nx / kZShapes[i].w);
       if (cap >= xtasks && cap <= 2 * xtasks && zfwd_shape_ok(i)) fsh.push_back(i);
       if (kZShapes[i].nt == 1 && kZShapes[i].nth <= 640) ash.push_back(i);
     }
@@ -1336,31 +1341,87 @@ void clamp_tails(const double* w, int p, float* EL, float* ER) {
   }
 }
 
+// Zero the outer taps of a factor while their summed magnitude, per side,
+// stays within 2^-27 of the factor's: below Float32 resolution of every
+// output (the two sides and two factors of a plane leave out at most 2^-25 of
+// its mass, against the 2^-24 rounding of one Float32 operation).
+// SPECT_ZTRIM=0 keeps every tap.
+void trim_taps(double* w, int n) {
+  double s = 0;
+  for (int i = 0; i < n; ++i) s += std::fabs(w[i]);
+  const double lim = std::ldexp(s, -27);
+  double acc = 0;
+  for (int i = 0; i < n; ++i) {
+    acc += std::fabs(w[i]);
+    if (acc > lim) break;
+    w[i] = 0;
+  }
+  acc = 0;
+  for (int i = n - 1; i >= 0; --i) {
+    acc += std::fabs(w[i]);
+    if (acc > lim) break;
+    w[i] = 0;
+  }
+}
+
+// taps of a pass row w[0, len) (len a multiple of 8) that a window pass runs:
+// 8-tap blocks from a 4-tap boundary, (first 4-tap block b4, block count n8)
+// covering every nonzero tap, 4 b4 + 8 n8 <= len
+void tap_range(const float* w, int len, int* b4, int* n8) {
+  int lo = 0, hi = len - 1;
+  while (lo < len && w[lo] == 0.f) ++lo;
+  while (hi > lo && w[hi] == 0.f) --hi;
+  if (lo >= len) {  // no tap (cannot happen for a plane factor)
+    *b4 = 0;
+    *n8 = 0;
+    return;
+  }
+  int b = lo / 4, n = (hi + 1 - 4 * b + 7) / 8;
+  if (4 * b + 8 * n > len) --b;  // 4 past the end: start 4 taps earlier (zeros)
+  *b4 = b;
+  *n8 = n;
+}
+
 // zpath launch shapes (no 1024-thread shape: it leaves too few registers):
 // forward -- the fewest thread slots holding every x task of a plane (ties:
 // more threads); adjoint -- the least padded x and z passes, one task per
 // thread and pass
+// shapes allowed by the geometry and by SPECT_ZW=8|16 (fixes the task width)
+bool zshape_allowed(const ZGeom& g, int i) {
+  const char* e = std::getenv("SPECT_ZW");
+  const int force = e ? std::atoi(e) : 0;
+  return zshape_fits(g, i) && (force == 0 || kZShapes[i].w == force);
+}
+// forward: the widest tasks, then the least thread capacity holding all x
+// tasks (their outputs stay in registers), then more threads
 int zpick_fwd(const ZGeom& g) {
-  const int xtasks = g.nz * (g.nx / 8);
   int best = -1;
   for (int i = 0; i < kZNShapes; ++i) {
-    const int cap = kZShapes[i].nt * kZShapes[i].nth;
-    if (cap < xtasks || !zfwd_shape_ok(i)) continue;
-    if (best < 0 || cap < kZShapes[best].nt * kZShapes[best].nth ||
-        (cap == kZShapes[best].nt * kZShapes[best].nth && kZShapes[i].nth > kZShapes[best].nth))
+    if (!zfwd_shape_ok(i) || !zshape_allowed(g, i)) continue;
+    const ZShape& s = kZShapes[i];
+    const int cap = s.nt * s.nth;
+    if (cap < g.nz * (g.nx / s.w)) continue;
+    if (best < 0) {
       best = i;
+      continue;
+    }
+    const ZShape& b = kZShapes[best];
+    if (s.w > b.w || (s.w == b.w && (cap < b.nt * b.nth || (cap == b.nt * b.nth && s.nth > b.nth)))) best = i;
   }
   return best;
 }
+// adjoint: one task per thread per pass round; the least padded work in
+// 8-output units (x and z tasks, rounded up to whole rounds), wider tasks on
+// ties
 int zpick_adj(const ZGeom& g) {
-  const long long xt = (long long)g.nz * (g.nx / 8), zt = (long long)g.nx * ((g.nz + 7) / 8);
   int best = -1;
   long long bc = 0;
   for (int i = 0; i < kZNShapes; ++i) {
-    const int nth = kZShapes[i].nth;
-    if (kZShapes[i].nt != 1 || nth > 640) continue;
-    const long long c = nth * ((xt + nth - 1) / nth + (zt + nth - 1) / nth);
-    if (best < 0 || c < bc) {
+    const ZShape& s = kZShapes[i];
+    if (s.nt != 1 || s.nth > 640 || !zshape_allowed(g, i)) continue;
+    const long long xt = (long long)g.nz * (g.nx / s.w), zt = (long long)g.nx * ((g.nz + s.w - 1) / s.w);
+    const long long c = s.nth * ((xt + s.nth - 1) / s.nth + (zt + s.nth - 1) / s.nth) * (s.w / 8);
+    if (best < 0 || c < bc || (c == bc && s.w > kZShapes[best].w)) {
       best = i;
       bc = c;
     }
@@ -1449,8 +1510,9 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     if (cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess)
       zcand = interpmeth == SPECT_INTERP_TWO && sep_host && !only_fft && !(zenv && zenv[0] == '0') && nx % 8 == 0 &&
-              zg.nzp <= 256 && zpick_fwd(zg) >= 0 && zpick_adj(zg) >= 0 && zfwd_smem(zg) <= (size_t)optin &&
-              zadj_smem(zg) <= (size_t)optin && opts.atten_cache != 0;
+              zg.zpw <= 72 && zg.xpw <= 72 &&  // pass rows of at most 9 blocks of 8 taps
+              zg.nzp <= 256 && zpick_fwd(zg) >= 0 && zpick_adj(zg) >= 0 && zfwd_smem(zg, 1) <= (size_t)optin &&
+              zadj_smem(zg, 1) <= (size_t)optin && opts.atten_cache != 0;
     cudaGetLastError();
   }
   // attenuation cache: on when it fits a quarter of the free device memory
@@ -1484,8 +1546,16 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     p->izN = (size_t)zg.L * zg.L * zg.nzp;
     p->zshape_fwd = zpick_fwd(zg);
     p->zshape_adj = zpick_adj(zg);
-    p->zfwd_smem_b = zfwd_smem(zg);
-    p->zadj_smem_b = zadj_smem(zg);
+    // double-buffered adjoint x pass where it fits (SPECT_ZADJ_BUFFERS=1: one buffer)
+    const char* nwa_env = std::getenv("SPECT_ZADJ_BUFFERS");
+    p->zg.nwa = (zadj_smem(zg, 2) <= p->max_smem && !(nwa_env && nwa_env[0] == '1')) ? 2 : 1;
+    // one forward staging buffer (SPECT_ZFWD_STAGES=2: two where they fit;
+    // measured slower at 128x128x80: the shared-memory carve-out takes L1
+    // from the gather's image reads)
+    const char* nsf_env = std::getenv("SPECT_ZFWD_STAGES");
+    p->zg.nsf = (zfwd_smem(zg, 2) <= p->max_smem && nsf_env && nsf_env[0] == '2') ? 2 : 1;
+    p->zfwd_smem_b = zfwd_smem(p->zg, p->zg.nsf);
+    p->zadj_smem_b = zadj_smem(p->zg, p->zg.nwa);
     const cudaError_t ze = zpath_setup((int)p->max_smem);
     if (ze != cudaSuccess) return bail(fail(SPECT_ERR_CUDA, std::string("fused kernel setup: ") + cudaGetErrorString(ze)));
   }
@@ -1725,9 +1795,14 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     std::vector<float> H((size_t)p->nset * ny * 2 * hs, 0.f), Tl((size_t)p->nset * ny * ts, 0.f);
     const bool ok = sep_host;
     std::vector<float> Hz, Ez;
+    std::vector<int> Rz;
+    std::vector<double> at(px), bt(pz);
+    const char* trim_env = std::getenv("SPECT_ZTRIM");
+    const bool trim = !(trim_env && trim_env[0] == '0');
     if (ok && p->zpath) {
       Hz.assign((size_t)p->nset * ny * 2 * zg.hs, 0.f);
       Ez.assign((size_t)p->nset * ny * 2 * zg.ts, 0.f);
+      Rz.assign((size_t)p->nset * ny * 8, 0);
     }
     for (int u = 0; ok && u < p->nset; ++u)
       for (int y = 0; y < ny; ++y) {
@@ -1744,24 +1819,42 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
         fold_tails(a, hxs, trow, trow + hxs);
         fold_tails(b, hzs, trow + 2 * hxs, trow + 2 * hxs + hzs);
         if (!Hz.empty()) {
-          // fused path: [fwd z | fwd x | adj z | adj x], each shifted right by
-          // its data offset minus the half width; tails [ELz ERz ELx ERx |
-          // cLx cRx cLz cRz]
+          // fused path, from the trimmed factors: [fwd z | fwd x | adj z |
+          // adj x], each shifted right by its data offset minus the half
+          // width; tails [ELz ERz ELx ERx | cLx cRx cLz cRz]; the tap-block
+          // range of each pass
+          std::copy(a, a + px, at.begin());
+          std::copy(b, b + pz, bt.begin());
+          if (trim) {
+            trim_taps(at.data(), px);
+            trim_taps(bt.data(), pz);
+          }
           const int sz = zg.R0 - zg.hz, sx = zg.C0 - zg.hx;
           float* zr = Hz.data() + ((size_t)u * ny + y) * 2 * zg.hs;
-          for (int m = 0; m < pz; ++m) zr[sz + m] = (float)b[pz - 1 - m];
-          for (int m = 0; m < px; ++m) zr[zg.zpw + sx + m] = (float)a[px - 1 - m];
-          for (int m = 0; m < pz; ++m) zr[zg.hs + sz + m] = (float)b[m];
-          for (int m = 0; m < px; ++m) zr[zg.hs + zg.zpw + sx + m] = (float)a[m];
+          for (int m = 0; m < pz; ++m) zr[sz + m] = (float)bt[pz - 1 - m];
+          for (int m = 0; m < px; ++m) zr[zg.zpw + sx + m] = (float)at[px - 1 - m];
+          for (int m = 0; m < pz; ++m) zr[zg.hs + sz + m] = (float)bt[m];
+          for (int m = 0; m < px; ++m) zr[zg.hs + zg.zpw + sx + m] = (float)at[m];
           float* er = Ez.data() + ((size_t)u * ny + y) * 2 * zg.ts;
-          clamp_tails(b, pz, er, er + hzs);
-          clamp_tails(a, px, er + 2 * hzs, er + 2 * hzs + hxs);
-          std::memcpy(er + zg.ts, trow, sizeof(float) * (2 * hxs + 2 * hzs));
+          clamp_tails(bt.data(), pz, er, er + hzs);
+          clamp_tails(at.data(), px, er + 2 * hzs, er + 2 * hzs + hxs);
+          fold_tails(at.data(), hxs, er + zg.ts, er + zg.ts + hxs);
+          fold_tails(bt.data(), hzs, er + zg.ts + 2 * hxs, er + zg.ts + 2 * hxs + hzs);
+          for (int m = 0; m < pz; ++m) p->ztaps[0] += bt[m] != 0.0 ? 1.0 : 0.0;
+          for (int m = 0; m < px; ++m) p->ztaps[1] += at[m] != 0.0 ? 1.0 : 0.0;
+          int* rr = Rz.data() + ((size_t)u * ny + y) * 8;
+          tap_range(zr, zg.zpw, rr, rr + 1);
+          tap_range(zr + zg.zpw, zg.xpw, rr + 2, rr + 3);
+          tap_range(zr + zg.hs, zg.zpw, rr + 4, rr + 5);
+          tap_range(zr + zg.hs + zg.zpw, zg.xpw, rr + 6, rr + 7);
         }
       }
     if (!Hz.empty()) {
+      p->ztaps[0] /= (double)p->nset * ny;
+      p->ztaps[1] /= (double)p->nset * ny;
       if ((st = dalloc(p, &p->d_Hz, Hz.size())) || (st = up(p->d_Hz, Hz.data(), sizeof(float) * Hz.size())) ||
-          (st = dalloc(p, &p->d_Ez, Ez.size())) || (st = up(p->d_Ez, Ez.data(), sizeof(float) * Ez.size())))
+          (st = dalloc(p, &p->d_Ez, Ez.size())) || (st = up(p->d_Ez, Ez.data(), sizeof(float) * Ez.size())) ||
+          (st = dalloc(p, &p->d_Rz, Rz.size())) || (st = up(p->d_Rz, Rz.data(), sizeof(int) * Rz.size())))
         return bail(st);
     }
     if (ok) {
@@ -1836,6 +1929,13 @@ int spect_plan_conv_kernels(spect_plan_t p, int out[4]) {
 int spect_plan_fused(spect_plan_t p, int* fused) {
   if (!p || !fused) return fail(SPECT_ERR_ARG, "null pointer argument");
   *fused = p->zpath;
+  return SPECT_OK;
+}
+
+int spect_plan_fused_taps(spect_plan_t p, double* taps) {
+  if (!p || !taps) return fail(SPECT_ERR_ARG, "null pointer argument");
+  taps[0] = p->zpath ? p->ztaps[0] : (double)p->pz;
+  taps[1] = p->zpath ? p->ztaps[1] : (double)p->px;
   return SPECT_OK;
 }
 

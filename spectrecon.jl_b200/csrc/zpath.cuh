@@ -38,13 +38,18 @@
 // out[i] = sum_{m<p} w[m] in[clamp(i - h + m)] with the reversed factor w
 // (the plan factors each PSF plane as a[d] b[e]).  Here the input line sits
 // zero-padded in shared memory, data starting at an offset D0 = h rounded up
-// to 4, and the weights are shifted right by D0 - h, so an 8-output task reads
-// a window of 16-byte-aligned float4s; the clamped boundary is added as tail
-// terms: the edge value times EL[i] = sum_{m < h - i} w[m] (i < h) or
-// ER[n-1-i] = sum_{m > h + n-1-i} w[m] (i > n-1-h).  The adjoint passes are the
-// zero-padded correlations with the factors themselves plus the folded padding
-// at the two ends (cL_k, cR_k: sums of the factor beyond k), as the reference's
-// padding adjoint does.
+// to 4, and the weights are shifted right by D0 - h, so a task of W = 8 or 16
+// consecutive outputs reads a window of 16-byte-aligned float4s; the clamped
+// boundary is added as tail terms: the edge value times EL[i] =
+// sum_{m < h - i} w[m] (i < h) or ER[n-1-i] = sum_{m > h + n-1-i} w[m]
+// (i > n-1-h).  The adjoint passes are the zero-padded correlations with the
+// factors themselves plus the folded padding at the two ends (cL_k, cR_k:
+// sums of the factor beyond k), as the reference's padding adjoint does.
+// The plan zeroes the outer taps of each factor whose summed magnitude per
+// side is within 2^-27 of the factor's (below Float32 resolution; a narrow
+// Gaussian plane keeps a few of its p taps) and every table, tails and folds
+// included, comes from those factors; per plane and pass a range table gives
+// the 8-tap blocks that hold the kept taps, and only those are run.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -57,56 +62,57 @@ namespace spect {
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 
-// 8 taps of one 8-output task: o[k] += w[s] e[s + k], with the block's
-// weights (w0, w1) and e = (p, q, r, t) the 16 consecutive window elements
-// starting at the block's first tap
-__device__ __forceinline__ void zfma8(float4 w0, float4 w1, float4 p, float4 q, float4 r, float4 t, float (&o)[8]) {
-  const float ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-  const float e[16] = {p.x, p.y, p.z, p.w, q.x, q.y, q.z, q.w, r.x, r.y, r.z, r.w, t.x, t.y, t.z, t.w};
+// one W-output task (W = 8 or 16) over a zero-padded line, the taps
+// m in [4 b4, 4 b4 + 8 nblk) in blocks of 8 (nblk <= 9): o[k] += sum_m w[m]
+// line[k + m] (line and w 16-byte aligned; reads line[4 b4, 4 b4 + 8 nblk +
+// W)).  Fully unrolled with a uniform early exit; the window elements are
+// named by constant indices (registers, no moves): per block two new quads
+// of the line and two weight quads feed 8 W FMAs.  Every output sums its
+// taps in ascending m, so W does not change the result.
+template <int W>
+__device__ __forceinline__ void zpassw(const float* __restrict__ w, int b4, int nblk, const float* line,
+                                       float (&o)[W]) {
+  w += 4 * b4;
+  line += 4 * b4;
+  float e[W + 8 * 9];
 #pragma unroll
-  for (int s = 0; s < 8; ++s)
+  for (int i = 0; i < W / 4; ++i) {
+    const float4 q = ld4(line + 4 * i);
+    e[4 * i] = q.x;
+    e[4 * i + 1] = q.y;
+    e[4 * i + 2] = q.z;
+    e[4 * i + 3] = q.w;
+  }
 #pragma unroll
-    for (int k = 0; k < 8; ++k) o[k] = fmaf(ws[s], e[s + k], o[k]);
+  for (int k = 0; k < 9; ++k) {
+    if (k >= nblk) break;
+    const float4 q0 = ld4(line + 8 * k + W), q1 = ld4(line + 8 * k + W + 4);
+    e[8 * k + W] = q0.x;
+    e[8 * k + W + 1] = q0.y;
+    e[8 * k + W + 2] = q0.z;
+    e[8 * k + W + 3] = q0.w;
+    e[8 * k + W + 4] = q1.x;
+    e[8 * k + W + 5] = q1.y;
+    e[8 * k + W + 6] = q1.z;
+    e[8 * k + W + 7] = q1.w;
+    const float4 w0 = ld4(w + 8 * k), w1 = ld4(w + 8 * k + 4);
+    const float ws[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+    for (int s2 = 0; s2 < 8; ++s2)
+#pragma unroll
+      for (int j = 0; j < W; ++j) o[j] = fmaf(ws[s2], e[8 * k + s2 + j], o[j]);
+  }
 }
 
-// one 8-output task over a zero-padded line, the window in nblk blocks of 8
-// taps (nblk <= 9): o[k] += sum_{m < 8 nblk} w[m] line[k + m] (line and w
-// 16-byte aligned; reads line[0, 8 nblk + 8)).  Fully unrolled with a uniform
-// early exit: the window quads alternate between two register pairs by name
-// (no loop counter or register moves), and the next block's weights are
-// loaded one block ahead, so a block's FMAs never start by waiting for them
-// (PF = false: loaded at the block, for callers short of registers).
-template <bool PF = true>
-__device__ __forceinline__ void zpassu(const float* __restrict__ w, int nblk, const float* line, float (&o)[8]) {
-  float4 a = ld4(line), b = ld4(line + 4), c, d;
-  float4 wa0 = ld4(w), wa1 = ld4(w + 4), wb0, wb1;
+// sum_{k < n} c[k] v[step k] for n <= 36 (a half width of a row of at most
+// 72 taps): predicated and fully unrolled, so every load is issued at once,
+// into four partial sums over k mod 4 added as (s0 + s1) + (s2 + s3)
+__device__ __forceinline__ float zfold(const float* c, const float* v, int step, int n) {
+  float s[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-  for (int k = 0; k < 10; k += 2) {
-    if (k >= nblk) break;
-    c = ld4(line + 8 * k + 8);
-    d = ld4(line + 8 * k + 12);
-    if (PF && k + 1 < nblk) {
-      wb0 = ld4(w + 8 * k + 8);
-      wb1 = ld4(w + 8 * k + 12);
-    }
-    if (!PF && k > 0) {
-      wa0 = ld4(w + 8 * k);
-      wa1 = ld4(w + 8 * k + 4);
-    }
-    zfma8(wa0, wa1, a, b, c, d, o);
-    if (k + 1 >= nblk) break;
-    a = ld4(line + 8 * k + 16);
-    b = ld4(line + 8 * k + 20);
-    if (PF && k + 2 < nblk) {
-      wa0 = ld4(w + 8 * k + 16);
-      wa1 = ld4(w + 8 * k + 20);
-    }
-    if (!PF) {
-      wb0 = ld4(w + 8 * k + 8);
-      wb1 = ld4(w + 8 * k + 12);
-    }
-    zfma8(wb0, wb1, c, d, a, b, o);
-  }
+  for (int k = 0; k < 36; ++k)
+    if (k < n) s[k & 3] = fmaf(c[k], v[step * k], s[k & 3]);
+  return (s[0] + s[1]) + (s[2] + s[3]);
 }
 
 // q = t / n for 0 <= t < 2^20, 1 <= n <= 4096, with r = 1/n rounded to float:
@@ -243,340 +249,455 @@ __global__ void __launch_bounds__(256) k_zatten(ZGeom g, const float* __restrict
 }
 
 // ------------------------------------------------------------------------
-// k_zfwd<NT, NTH>: persistent forward, one block per SM, NTH threads; NT
-// x-pass tasks per thread, all of a plane's x tasks resident
-// (NT * NTH >= nz * nx / 8) since their outputs accumulate over the chunk.
-// Per plane: wait for the staged attenuation plane and weights, sample
-// geometry of the plane's nx rotated-grid columns, gather into ZB, z pass
-// into XB, x pass into registers (three block barriers per plane).
-template <int NT, int NTH>
+// k_zfwd<NT, NTH, W>: persistent forward, one block per SM, NTH threads; NT
+// x-pass tasks of W outputs per thread, all of a plane's x tasks resident
+// (NT * NTH >= nz * nx / W) since their outputs accumulate over the chunk.
+// The block walks its planes in sequence; the attenuation plane and weights
+// of the next nsf planes are bulk-copied while plane p is worked on (stage
+// q % nsf holds plane q).  Two block barriers per plane: phase A runs the z
+// pass of plane p (ZB -> XB) and the sample geometry of plane p + 1; phase B
+// the x pass of plane p (XB -> registers) and the gather of plane p + 1
+// (rotated, attenuated image -> ZB).
+template <int NT, int NTH, int W>
 __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
   extern __shared__ float4 smem4[];
   const ZGeom& g = a.g;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts, nsf = g.nsf;
   float* const base = reinterpret_cast<float*>(smem4);
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);
-  float* const sA = base + 4;                   // attenuation plane [x][nzp]
-  float* const sW = sA + (size_t)nx * nzp;      // weights then tails (staging)
-  float* const Hw0 = sW + hs + ts;              // working weights, two planes
-  float2* const PA = reinterpret_cast<float2*>(Hw0 + 2 * (hs + ts));
-  float2* const PB = PA + nx;
-  float4* const geoW = reinterpret_cast<float4*>(PB + ny);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);  // nsf barriers
+  const int sts = nx * nzp + hs + ts;  // stage: attenuation plane [x][nzp], weights, tails
+  float* const stage = base + 4;
+  float* const Hw0 = stage + nsf * sts;           // working weights, two planes
+  float4* const geoW = reinterpret_cast<float4*>(Hw0 + 2 * (hs + ts));
   int* const geoO = reinterpret_cast<int*>(geoW + nx);
   float* const ZB = reinterpret_cast<float*>(geoO + zround(nx, 4));  // [x][ast], data rows R0..R0+nz-1
   float* const XB = ZB + (size_t)nx * g.ast;                          // [z][bs], data columns C0..C0+nx-1
   const int tid = threadIdx.x;
   const int nitems = a.nv * a.nchunks;
+  const float rnc = 1.0f / a.nchunks;
+  auto slot_of = [&](int item) { return zdiv(item, rnc); };             // item / nchunks (items < 2^20)
+  auto chunk_of = [&](int item) { return item - zdiv(item, rnc) * a.nchunks; };
   const unsigned abytes = (unsigned)((size_t)nx * nzp * sizeof(float));
-  auto issue = [&](int item, int y) {  // one thread: attenuation plane, weights, tails of plane y
-    const int sl = item / a.nchunks, v = a.vidx[sl], set = a.viewset[v];
+  auto issue = [&](int item, int y, int s) {  // one thread: attenuation plane, weights, tails of plane y
+    const int sl = slot_of(item), v = a.vidx[sl], set = a.viewset[v];
+    float* sA = stage + s * sts;
+    float* sW = sA + nx * nzp;
     fence_proxy_async();
-    mbar_expect(bar, abytes + (unsigned)((hs + ts) * sizeof(float)));
-    bulk_copy(bar, sA, a.att + ((size_t)v * ny + y) * nx * nzp, abytes);
-    bulk_copy(bar, sW, a.H + ((size_t)set * ny + y) * (2 * hs), (unsigned)(hs * sizeof(float)));
-    bulk_copy(bar, sW + hs, a.E + ((size_t)set * ny + y) * (2 * ts), (unsigned)(ts * sizeof(float)));
+    mbar_expect(&bar[s], abytes + (unsigned)((hs + ts) * sizeof(float)));
+    bulk_copy(&bar[s], sA, a.att + ((size_t)v * ny + y) * nx * nzp, abytes);
+    bulk_copy(&bar[s], sW, a.H + ((size_t)set * ny + y) * (2 * hs), (unsigned)(hs * sizeof(float)));
+    bulk_copy(&bar[s], sW + hs, a.E + ((size_t)set * ny + y) * (2 * ts), (unsigned)(ts * sizeof(float)));
+  };
+  auto next = [&](int& item, int& y) {
+    const int yend = min(ny, chunk_of(item) * a.chunkY + a.chunkY);
+    if (y + 1 < yend) {
+      ++y;
+    } else {
+      item += gridDim.x;
+      y = chunk_of(item) * a.chunkY;
+    }
   };
   // the padded buffers start zero; only their data rows / columns are written later
   for (size_t k = tid; k < (size_t)nx * g.ast + (size_t)nz * g.bs; k += NTH) ZB[k] = 0.f;
+  int i0 = blockIdx.x, y0 = (blockIdx.x % a.nchunks) * a.chunkY;  // plane p
+  int i1 = i0, y1 = y0;
+  next(i1, y1);  // p + 1
+  int iq = i1, yq = y1;  // the next plane to issue
+  unsigned pend = 0u;    // stages with a copy issued and not yet waited for (same in every thread)
   if (tid == 0) {
-    mbar_init(bar);
-    if ((int)blockIdx.x < nitems) issue(blockIdx.x, ((int)blockIdx.x % a.nchunks) * a.chunkY);
+    for (int s = 0; s < nsf; ++s) mbar_init(&bar[s]);
+    if (i0 < nitems) issue(i0, y0, 0);
+  }
+  pend = 1u;
+  if (nsf > 1) {
+    if (tid == 0 && iq < nitems) issue(iq, yq, 1);
+    if (iq < nitems) pend |= 2u;
+    next(iq, yq);
   }
   __syncthreads();
-  const int nzb = (nz + 7) / 8, ztasks = nx * nzb, nz4 = (nz + 3) / 4, units = nx * nz4;
-  const int xtasks = nz * (nx / 8);
+  if (!(i0 < nitems)) return;
+  const int nzb = (nz + W - 1) / W, ztasks = nx * nzb, nz4 = (nz + 3) / 4, units = nx * nz4;
+  const int xtasks = nz * (nx / W);
   const size_t Lz = (size_t)g.L * nzp;
   const int ast = g.ast, bs = g.bs, R0 = g.R0, C0 = g.C0, hz = g.hz, hx = g.hx;
-  const int zblk = g.zpw / 8, xblk = g.xpw / 8, zpw = g.zpw;
+  const int zpw = g.zpw;
   const float rnx = 1.0f / nx, rnz = 1.0f / nz, rnz4 = 1.0f / nz4;
-  unsigned phase = 0;
-  int yb = 0;  // working-weight buffer of the current plane
-  float acc[NT][8];
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int slot = item / a.nchunks, ch = item - slot * a.nchunks;
-    const int v = a.vidx[slot];
-    const int y0 = ch * a.chunkY, y1 = min(ny, y0 + a.chunkY);
-    const float4 r = a.rot[v];
-    const float cs = r.x, sn = r.y;
-    const bool ident = r.z != 0.f;
-    // position tables of this view, the products of RotPos::pos (the
-    // previous item's geometry was done before its last barrier)
-    for (int e = tid; e < nx + ny; e += NTH) {
-      const int o = e < nx ? e : e - nx;
-      const float d = __fsub_rn((float)o, g.c0);
-      if (e < nx) PA[o] = make_float2(__fmul_rn(cs, d), __fmul_rn(sn, d));
-      else PB[o] = make_float2(__fmul_rn(sn, d), __fmul_rn(cs, d));
+  unsigned phases = 0u;  // parity of each barrier's next wait
+  // wait for stage s; false (every thread) when a wait gave up, after the
+  // copies in flight have landed
+  auto staged = [&](int s) {
+    const bool ok = mbar_wait(&bar[s], (phases >> s) & 1u);
+    if (ok) {
+      phases ^= 1u << s;
+      pend &= ~(1u << s);
     }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < NT; ++i)
-#pragma unroll
-      for (int k = 0; k < 8; ++k) acc[i][k] = 0.f;
-    for (int y = y0; y < y1; ++y) {
-      const bool ok = mbar_wait(bar, phase);
-      phase ^= 1u;
-      float* const Hw = Hw0 + yb * (hs + ts);
-      // sample geometry of plane y, one rotated-grid column per thread
-      if (tid < nx) {
-        int j1 = tid, j2 = y;
-        float4 w = make_float4(1.f, 0.f, 0.f, 0.f);
-        if (!ident) {
-          const float2 pa = PA[tid], pb = PB[y];
-          const float s1 = __fadd_rn(g.c0, __fsub_rn(pa.x, pb.x)), s2 = __fadd_rn(g.c0, __fadd_rn(pa.y, pb.y));
-          const float f1 = floorf(s1), f2 = floorf(s2);
-          const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
-          const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
-          j1 = (int)f1;
-          j2 = (int)f2;
-          w = make_float4(__fmul_rn(u1, u2), __fmul_rn(t1, u2), __fmul_rn(u1, t2), __fmul_rn(t1, t2));
-          if (j1 < -g.pad || j1 > nx + g.pad - 2 || j2 < -g.pad || j2 > nx + g.pad - 2) {
-            j1 = j2 = 0;
-            w = make_float4(0.f, 0.f, 0.f, 0.f);
-          }
-        }
-        geoW[tid] = w;
-        geoO[tid] = ((j2 + g.pad) * g.L + j1 + g.pad) * nzp;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(a.err, 1);
+        for (int k = 0; k < nsf; ++k)
+          if ((pend >> k) & 1u) mbar_wait(&bar[k], (phases >> k) & 1u);
       }
-      for (int k = tid; k < hs + ts; k += NTH) Hw[k] = sW[k];
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) {
-          atomicExch(a.err, 1);
-          mbar_wait(bar, phase ^ 1u);
-        }
-        return;
-      }
-      // rotated, attenuated plane into ZB (column x, rows R0 + z), four z at a time
-      for (int u = tid; u < units; u += NTH) {
-        const int x = zdiv(u, rnz4), zg = u - x * nz4;
-        const float4 w = geoW[x];
-        const float* p = a.img + geoO[x] + 4 * zg;
-        const float4 t0 = ld4(p), t1 = ld4(p + nzp), t2 = ld4(p + Lz), t3 = ld4(p + Lz + nzp);
-        const float4 at = ld4(sA + x * nzp + 4 * zg);
-        float4 o;
-        o.x = __fmul_rn(fmaf(w.w, t3.x, fmaf(w.z, t2.x, fmaf(w.y, t1.x, __fmul_rn(w.x, t0.x)))), at.x);
-        o.y = __fmul_rn(fmaf(w.w, t3.y, fmaf(w.z, t2.y, fmaf(w.y, t1.y, __fmul_rn(w.x, t0.y)))), at.y);
-        o.z = __fmul_rn(fmaf(w.w, t3.z, fmaf(w.z, t2.z, fmaf(w.y, t1.z, __fmul_rn(w.x, t0.z)))), at.z);
-        o.w = __fmul_rn(fmaf(w.w, t3.w, fmaf(w.z, t2.w, fmaf(w.y, t1.w, __fmul_rn(w.x, t0.w)))), at.w);
-        st4(ZB + x * ast + R0 + 4 * zg, o);
-      }
-      __syncthreads();
-      if (tid == 0) {  // next plane of this block into the staging buffers
-        if (y + 1 < y1) issue(item, y + 1);
-        else if (item + (int)gridDim.x < nitems) issue(item + gridDim.x, ((item + (int)gridDim.x) % a.nchunks) * a.chunkY);
-      }
-      // z pass: task (x, z block) -> XB rows z, column C0 + x
-      const float* ELz = Hw + hs;
-      const float* ERz = ELz + hz;
-      for (int t = tid; t < ztasks; t += NTH) {
-        const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = 8 * zb;
-        float o[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) o[k] = 0.f;
-        const float* col = ZB + x * ast;
-        zpassu<(NT <= 2)>(Hw, zblk, col + z0, o);
-        if (z0 < hz) {  // clamped rows above the plane
-          const float e0 = col[R0];
-#pragma unroll
-          for (int k = 0; k < 8; ++k)
-            if (z0 + k < hz) o[k] = fmaf(ELz[z0 + k], e0, o[k]);
-        }
-        if (z0 + 8 > nz - hz) {  // clamped rows below
-          const float e1 = col[R0 + nz - 1];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int kk = nz - 1 - z0 - k;
-            if (kk >= 0 && kk < hz) o[k] = fmaf(ERz[kk], e1, o[k]);
-          }
-        }
-        float* xo = XB + z0 * bs + C0 + x;
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
-          if (z0 + k < nz) xo[k * bs] = o[k];
-      }
-      __syncthreads();
-      // x pass, accumulated over the chunk
-      const float* ELx = ERz + hz;
-      const float* ERx = ELx + hx;
-#pragma unroll
-      for (int i = 0; i < NT; ++i) {
-        const int t = tid + i * NTH;
-        if (t < xtasks) {
-          const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
-          const float* row = XB + z * bs;
-          zpassu<(NT <= 2)>(Hw + zpw, xblk, row + x0, acc[i]);
-          if (x0 < hx) {
-            const float e0 = row[C0];
-#pragma unroll
-            for (int k = 0; k < 8; ++k)
-              if (x0 + k < hx) acc[i][k] = fmaf(ELx[x0 + k], e0, acc[i][k]);
-          }
-          if (x0 + 8 > nx - hx) {
-            const float e1 = row[C0 + nx - 1];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              const int kk = nx - 1 - x0 - k;
-              if (kk < hx) acc[i][k] = fmaf(ERx[kk], e1, acc[i][k]);
-            }
-          }
-        }
-      }
-      yb ^= 1;
+      return false;
     }
-    // partial view of this chunk: part[slot][ch][z][x]
-    float* out = a.part + ((size_t)slot * a.nchunks + ch) * nz * nx;
+    return true;
+  };
+  // sample geometry of plane (item, y), one rotated-grid column per thread:
+  // the position arithmetic of RotPos::pos with the view's (cos, sin)
+  auto geometry = [&](int item, int y) {
+    if (tid < nx) {
+      const float4 r = a.rot[a.vidx[slot_of(item)]];
+      int j1 = tid, j2 = y;
+      float4 w = make_float4(1.f, 0.f, 0.f, 0.f);
+      if (r.z == 0.f) {
+        const float cs = r.x, sn = r.y;
+        const float d1 = __fsub_rn((float)tid, g.c0), d2 = __fsub_rn((float)y, g.c0);
+        const float s1 = __fadd_rn(g.c0, __fsub_rn(__fmul_rn(cs, d1), __fmul_rn(sn, d2)));
+        const float s2 = __fadd_rn(g.c0, __fadd_rn(__fmul_rn(sn, d1), __fmul_rn(cs, d2)));
+        const float f1 = floorf(s1), f2 = floorf(s2);
+        const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
+        const float u1 = __fsub_rn(1.0f, t1), u2 = __fsub_rn(1.0f, t2);
+        j1 = (int)f1;
+        j2 = (int)f2;
+        w = make_float4(__fmul_rn(u1, u2), __fmul_rn(t1, u2), __fmul_rn(u1, t2), __fmul_rn(t1, t2));
+        if (j1 < -g.pad || j1 > nx + g.pad - 2 || j2 < -g.pad || j2 > nx + g.pad - 2) {
+          j1 = j2 = 0;
+          w = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      geoW[tid] = w;
+      geoO[tid] = ((j2 + g.pad) * g.L + j1 + g.pad) * nzp;
+    }
+  };
+  // staged weights of stage s into working buffer hb; rotated, attenuated
+  // plane into ZB (column x, rows R0 + z), four z at a time
+  auto gather = [&](int s, int hb) {
+    const float* const sA = stage + s * sts;
+    const float* const sW = sA + nx * nzp;
+    float* const Hw = Hw0 + hb * (hs + ts);
+    for (int k = tid; k < hs + ts; k += NTH) Hw[k] = sW[k];
+    for (int u = tid; u < units; u += NTH) {
+      const int x = zdiv(u, rnz4), zg = u - x * nz4;
+      const float4 w = geoW[x];
+      const float* p = a.img + geoO[x] + 4 * zg;
+      const float4 t0 = ld4(p), t1 = ld4(p + nzp), t2 = ld4(p + Lz), t3 = ld4(p + Lz + nzp);
+      const float4 at = ld4(sA + x * nzp + 4 * zg);
+      float4 o;
+      o.x = __fmul_rn(fmaf(w.w, t3.x, fmaf(w.z, t2.x, fmaf(w.y, t1.x, __fmul_rn(w.x, t0.x)))), at.x);
+      o.y = __fmul_rn(fmaf(w.w, t3.y, fmaf(w.z, t2.y, fmaf(w.y, t1.y, __fmul_rn(w.x, t0.y)))), at.y);
+      o.z = __fmul_rn(fmaf(w.w, t3.z, fmaf(w.z, t2.z, fmaf(w.y, t1.z, __fmul_rn(w.x, t0.z)))), at.z);
+      o.w = __fmul_rn(fmaf(w.w, t3.w, fmaf(w.z, t2.w, fmaf(w.y, t1.w, __fmul_rn(w.x, t0.w)))), at.w);
+      st4(ZB + x * ast + R0 + 4 * zg, o);
+    }
+  };
+  float acc[NT][W];
+#pragma unroll
+  for (int i = 0; i < NT; ++i)
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[i][k] = 0.f;
+  // the stage that plane p's copy used is free again: the plane nsf ahead
+  auto refill = [&](int s) {
+    if (iq < nitems) {
+      if (tid == 0) issue(iq, yq, s);
+      pend |= 1u << s;
+    }
+    next(iq, yq);
+  };
+  // prologue: plane p's geometry and staged data, its gather
+  geometry(i0, y0);
+  if (!staged(0)) return;
+  gather(0, 0);
+  __syncthreads();
+  refill(0);
+  int hb = 0, s1 = nsf > 1 ? 1 : 0;  // working-weight buffer of plane p, stage of plane p + 1
+  for (;;) {
+    const bool h1 = i1 < nitems;
+    const float* Hw = Hw0 + hb * (hs + ts);
+    const int4 rg = *reinterpret_cast<const int4*>(a.R + ((size_t)a.viewset[a.vidx[slot_of(i0)]] * ny + y0) * 8);
+    // phase A: z pass of p, task (x, z block) -> XB rows z, column C0 + x
+    const float* ELz = Hw + hs;
+    const float* ERz = ELz + hz;
+    for (int t = tid; t < ztasks; t += NTH) {
+      const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = W * zb;
+      float o[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) o[k] = 0.f;
+      const float* col = ZB + x * ast;
+      zpassw<W>(Hw, rg.x, rg.y, col + z0, o);
+      if (z0 < hz) {  // clamped rows above the plane
+        const float e0 = col[R0];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+          if (z0 + k < hz) o[k] = fmaf(ELz[z0 + k], e0, o[k]);
+      }
+      if (z0 + W > nz - hz) {  // clamped rows below
+        const float e1 = col[R0 + nz - 1];
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          const int kk = nz - 1 - z0 - k;
+          if (kk >= 0 && kk < hz) o[k] = fmaf(ERz[kk], e1, o[k]);
+        }
+      }
+      float* xo = XB + z0 * bs + C0 + x;
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        if (z0 + k < nz) xo[k * bs] = o[k];
+    }
+    if (h1) {
+      geometry(i1, y1);
+      if (!staged(s1)) return;
+    } else {
+      __syncthreads();
+    }
+    // phase B: x pass of p, accumulated over the chunk; gather of p + 1
+    const float* ELx = ERz + hz;
+    const float* ERx = ELx + hx;
 #pragma unroll
     for (int i = 0; i < NT; ++i) {
       const int t = tid + i * NTH;
       if (t < xtasks) {
-        const int xb = zdiv(t, rnz), z = t - xb * nz;
-        float* o = out + (size_t)z * nx + 8 * xb;
-        st4(o, make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]));
-        st4(o + 4, make_float4(acc[i][4], acc[i][5], acc[i][6], acc[i][7]));
+        const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = W * xb;
+        const float* row = XB + z * bs;
+        zpassw<W>(Hw + zpw, rg.z, rg.w, row + x0, acc[i]);
+        if (x0 < hx) {
+          const float e0 = row[C0];
+#pragma unroll
+          for (int k = 0; k < W; ++k)
+            if (x0 + k < hx) acc[i][k] = fmaf(ELx[x0 + k], e0, acc[i][k]);
+        }
+        if (x0 + W > nx - hx) {
+          const float e1 = row[C0 + nx - 1];
+#pragma unroll
+          for (int k = 0; k < W; ++k) {
+            const int kk = nx - 1 - x0 - k;
+            if (kk < hx) acc[i][k] = fmaf(ERx[kk], e1, acc[i][k]);
+          }
+        }
       }
     }
+    if (h1) gather(s1, hb ^ 1);
+    if (!h1 || i1 != i0) {  // p ends its item: partial view of the chunk, part[slot][ch][z][x]
+      const int slot = slot_of(i0), ch = i0 - slot * a.nchunks;
+      float* out = a.part + ((size_t)slot * a.nchunks + ch) * nz * nx;
+#pragma unroll
+      for (int i = 0; i < NT; ++i) {
+        const int t = tid + i * NTH;
+        if (t < xtasks) {
+          const int xb = zdiv(t, rnz), z = t - xb * nz;
+          float* o = out + (size_t)z * nx + W * xb;
+#pragma unroll
+          for (int k = 0; k < W; k += 4) st4(o + k, make_float4(acc[i][k], acc[i][k + 1], acc[i][k + 2], acc[i][k + 3]));
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k) acc[i][k] = 0.f;
+      }
+    }
+    if (!h1) break;
+    __syncthreads();
+    refill(s1);
+    i0 = i1;
+    y0 = y1;
+    next(i1, y1);
+    hb ^= 1;
+    s1 = nsf > 1 ? s1 ^ 1 : 0;
   }
 }
 
 // ------------------------------------------------------------------------
-// k_zadj<NT, NTH>: adjoint convolution; work items (slot, depth chunk); the
-// view is loaded zero-padded once per item; per plane the adjoint weights and
-// folds are bulk-copied two planes deep; x pass (view rows) -> WB, z pass (WB
-// columns) -> times the attenuation column (16-byte global loads issued at
-// the task's start) -> T.  NT only sets how the x tasks are interleaved.
-template <int NT, int NTH>
+// k_zadj<NT, NTH, W>: adjoint convolution (tasks of W outputs); work items (slot, depth chunk), the
+// block's planes walked in sequence.  Plane p's adjoint weights and folds are
+// bulk-copied three planes ahead (stage p % 3); its x pass (view rows) writes
+// the x-pass buffer WB[p % nwa] and its z pass (WB columns, times the
+// attenuation column read by 16-byte global loads at the task start) writes
+// T.  One phase between two block barriers runs the z pass of plane p and
+// the x pass of plane p + 1, so with two buffers each plane costs one barrier
+// (one more where plane p + 1 starts a new item: the view is reloaded; and,
+// with one buffer, one between the two passes).  NT only sets how the x
+// tasks are interleaved.
+template <int NT, int NTH, int W>
 __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   extern __shared__ float4 smem4[];
   const ZGeom& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts;
   float* const base = reinterpret_cast<float*>(smem4);
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);  // two barriers
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);  // three barriers
   const int sts = hs + ts;                 // one stage: weights, folds
-  float* const stage = base + 4;
-  float* const VB = stage + 2 * sts;
-  float* const WB = VB + (size_t)nz * g.bs;
+  float* const stage = base + 8;
+  float* const VB = stage + 3 * sts;
+  float* const WB0 = VB + (size_t)nz * g.bs;
+  const size_t wbs = g.nwa > 1 ? (size_t)nx * g.ast : 0;  // offset of the second buffer
   const int tid = threadIdx.x;
   const int nitems = a.nv * a.nchunks;
-  auto issue = [&](int item, int y, int b) {  // one thread
-    const int sl = item / a.nchunks, v = a.vidx[sl], set = a.viewset[v];
-    float* st = stage + b * sts;
+  const float rnc = 1.0f / a.nchunks;
+  auto slot_of = [&](int item) { return zdiv(item, rnc); };             // item / nchunks (items < 2^20)
+  auto chunk_of = [&](int item) { return item - zdiv(item, rnc) * a.nchunks; };
+  auto issue = [&](int item, int y, int s) {  // one thread
+    const int sl = slot_of(item), v = a.vidx[sl], set = a.viewset[v];
+    float* st = stage + s * sts;
     fence_proxy_async();
-    mbar_expect(&bar[b], (unsigned)((hs + ts) * sizeof(float)));
-    bulk_copy(&bar[b], st, a.H + ((size_t)set * ny + y) * (2 * hs) + hs, (unsigned)(hs * sizeof(float)));
-    bulk_copy(&bar[b], st + hs, a.E + ((size_t)set * ny + y) * (2 * ts) + ts, (unsigned)(ts * sizeof(float)));
+    mbar_expect(&bar[s], (unsigned)((hs + ts) * sizeof(float)));
+    bulk_copy(&bar[s], st, a.H + ((size_t)set * ny + y) * (2 * hs) + hs, (unsigned)(hs * sizeof(float)));
+    bulk_copy(&bar[s], st + hs, a.E + ((size_t)set * ny + y) * (2 * ts) + ts, (unsigned)(ts * sizeof(float)));
   };
   auto next = [&](int& item, int& y) {
-    const int yend = min(ny, (item % a.nchunks) * a.chunkY + a.chunkY);
+    const int yend = min(ny, chunk_of(item) * a.chunkY + a.chunkY);
     if (y + 1 < yend) {
       ++y;
     } else {
       item += gridDim.x;
-      y = (item % a.nchunks) * a.chunkY;
+      y = chunk_of(item) * a.chunkY;
     }
   };
   // WB rows outside the data rows stay zero
-  for (int x = tid / 32; x < nx; x += NTH / 32)
+  for (int x = tid / 32; x < g.nwa * nx; x += NTH / 32)
     for (int r = tid & 31; r < g.ast; r += 32)
-      if (r < g.R0 || r >= g.R0 + nz) WB[(size_t)x * g.ast + r] = 0.f;
-  int qi = blockIdx.x, qy = (blockIdx.x % a.nchunks) * a.chunkY;  // plane P0
-  int i1 = qi, y1q = qy;
-  next(i1, y1q);  // P1
+      if (r < g.R0 || r >= g.R0 + nz) WB0[(size_t)x * g.ast + r] = 0.f;
+  // planes p, p + 1, p + 2 and p + 3 (the next to issue)
+  int i0 = blockIdx.x, y0 = (blockIdx.x % a.nchunks) * a.chunkY;
+  int i1 = i0, y1 = y0;
+  next(i1, y1);
+  int i2 = i1, y2 = y1;
+  next(i2, y2);
+  int i3 = i2, y3 = y2;
+  next(i3, y3);
   if (tid == 0) {
     mbar_init(&bar[0]);
     mbar_init(&bar[1]);
-    if (qi < nitems) {
-      issue(qi, qy, 0);
-      if (i1 < nitems) issue(i1, y1q, 1);
-    }
+    mbar_init(&bar[2]);
+    if (i0 < nitems) issue(i0, y0, 0);
+    if (i1 < nitems) issue(i1, y1, 1);
+    if (i2 < nitems) issue(i2, y2, 2);
   }
   __syncthreads();
-  qi = i1;
-  qy = y1q;
-  next(qi, qy);  // P2: the next plane to issue
-  if (!((int)blockIdx.x < nitems)) return;
-  const int nzb = (nz + 7) / 8, ztasks = nx * nzb, xtasks = nz * (nx / 8);
+  if (!(i0 < nitems)) return;
+  unsigned pend = (i1 < nitems ? 7u : 1u) & (i2 < nitems ? 7u : 3u);  // copies issued, not yet waited for
+  unsigned phases = 0u;                                                  // parity of each barrier's next wait
+  auto wait = [&](int s) {
+    const bool ok = mbar_wait(&bar[s], (phases >> s) & 1u);
+    if (ok) {
+      phases ^= 1u << s;
+      pend &= ~(1u << s);
+    }
+    return ok;
+  };
+  auto give_up = [&]() {  // after a failed wait: flag it, let the copies in flight land
+    if (tid == 0) {
+      atomicExch(a.err, 1);
+      for (int s = 0; s < 3; ++s)
+        if ((pend >> s) & 1u) mbar_wait(&bar[s], (phases >> s) & 1u);
+    }
+  };
+  const int nzb = (nz + W - 1) / W, ztasks = nx * nzb, xtasks = nz * (nx / W);
   const int ast = g.ast, bs = g.bs, R0 = g.R0, C0 = g.C0, hz = g.hz, hx = g.hx;
-  const int zblk = g.zpw / 8, xblk = g.xpw / 8;
   const float rnx = 1.0f / nx, rnz = 1.0f / nz;
-  unsigned phases = 0u;
-  int b = 0;
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int slot = item / a.nchunks, ch = item - slot * a.nchunks;
-    const int v = a.vidx[slot];
-    const int y0 = ch * a.chunkY, y1 = min(ny, y0 + a.chunkY);
-    // the view, zero-padded (the previous item's passes ended at a barrier)
-    const float* V = a.views + (size_t)slot * nz * nx;
+  auto load_view = [&](int item) {  // the item's view, zero-padded
+    const float* V = a.views + (size_t)slot_of(item) * nz * nx;
     for (int z = tid / 32; z < nz; z += NTH / 32) {
-      float* row = VB + (size_t)z * g.bs;
-      for (int c = tid & 31; c < g.bs; c += 32) row[c] = (c >= g.C0 && c < g.C0 + nx) ? V[z * nx + c - g.C0] : 0.f;
+      float* row = VB + (size_t)z * bs;
+      for (int c = tid & 31; c < bs; c += 32) row[c] = (c >= C0 && c < C0 + nx) ? V[z * nx + c - C0] : 0.f;
     }
-    for (int y = y0; y < y1; ++y) {
-      const unsigned par = (phases >> b) & 1u;
-      if (__syncthreads_or(!mbar_wait(&bar[b], par))) {
-        if (tid == 0) {
-          atomicExch(a.err, 1);
-          mbar_wait(&bar[b], par);
-        }
-        return;
+  };
+  // x pass of the plane whose stage is st: task (z, x block) -> WB column x, row R0 + z
+  auto xpass = [&](const float* st, float* WB, int item, int y) {
+    const int2 rg = *reinterpret_cast<const int2*>(a.R + ((size_t)a.viewset[a.vidx[slot_of(item)]] * ny + y) * 8 + 6);
+    const float* ax = st + g.zpw;     // adjoint x weights (shifted)
+    const float* cLx = st + hs;       // folds
+    const float* cRx = cLx + hx;
+#pragma unroll
+    for (int i = 0; i < NT; ++i)
+      for (int t = tid + i * NTH; t < xtasks; t += NT * NTH) {
+        const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = W * xb;
+        const float* row = VB + z * bs;
+        float o[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) o[k] = 0.f;
+        zpassw<W>(ax, rg.x, rg.y, row + x0, o);
+        if (x0 == 0)
+          o[0] += zfold(cLx, row + C0, 1, hx);
+        if (x0 + W == nx)
+          o[W - 1] += zfold(cRx, row + C0 + nx - 1, -1, hx);
+        float* w = WB + x0 * ast + R0 + z;
+#pragma unroll
+        for (int k = 0; k < W; ++k) w[k * ast] = o[k];
       }
-      phases ^= 1u << b;
-      const float* st = stage + b * sts;
-      const float* az = st;             // adjoint z weights (shifted)
-      const float* ax = st + g.zpw;     // adjoint x weights (shifted)
-      const float* cLx = st + hs;       // folds
-      const float* cRx = cLx + g.hx;
-      const float* cLz = cRx + g.hx;
-      const float* cRz = cLz + g.hz;
-      // x pass: task (z, x block) -> WB column x, row R0 + z
+  };
+  // z pass of plane (item, y), stage st: task (x, z block) -> T column (x, y) of the slot
+  auto zpass = [&](const float* st, const float* WB, int item, int y) {
+    const int slot = slot_of(item), v = a.vidx[slot];
+    const int2 rg = *reinterpret_cast<const int2*>(a.R + ((size_t)a.viewset[v] * ny + y) * 8 + 4);
+    const float* az = st;             // adjoint z weights (shifted)
+    const float* cLz = st + hs + 2 * hx;
+    const float* cRz = cLz + hz;
+    const float* attv = a.att + (((size_t)v * ny + y) * nx) * nzp;
+    float* Tp = a.T + (((size_t)slot * ny + y) * nx) * nzp;
+    for (int t = tid; t < ztasks; t += NTH) {
+      const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = W * zb;
+      float4 at[W / 4];
 #pragma unroll
-      for (int i = 0; i < NT; ++i)
-        for (int t = tid + i * NTH; t < xtasks; t += NT * NTH) {
-          const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = 8 * xb;
-          const float* row = VB + z * bs;
-          float o[8];
+      for (int k = 0; k < W / 4; ++k) at[k] = ld4(attv + x * nzp + z0 + 4 * k);
+      const float* col = WB + x * ast;
+      float o[W];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) o[k] = 0.f;
-          zpassu(ax, xblk, row + x0, o);
-          if (x0 == 0)
-            for (int k = 0; k < hx; ++k) o[0] = fmaf(cLx[k], row[C0 + k], o[0]);
-          if (x0 + 8 == nx)
-            for (int k = 0; k < hx; ++k) o[7] = fmaf(cRx[k], row[C0 + nx - 1 - k], o[7]);
-          float* w = WB + x0 * ast + R0 + z;
+      for (int k = 0; k < W; ++k) o[k] = 0.f;
+      zpassw<W>(az, rg.x, rg.y, col + z0, o);
+      if (z0 == 0)
+        o[0] += zfold(cLz, col + R0, 1, hz);
+      if (z0 <= nz - 1 && nz - 1 < z0 + W) {
+        const int kz = nz - 1 - z0;
+        const float s = zfold(cRz, col + R0 + nz - 1, -1, hz);
 #pragma unroll
-          for (int k = 0; k < 8; ++k) w[k * ast] = o[k];
-        }
-      __syncthreads();
-      // z pass: task (x, z block) -> T column (x, y) of the slot
-      const float* attv = a.att + (((size_t)v * ny + y) * nx) * nzp;
-      float* Tp = a.T + (((size_t)slot * ny + y) * nx) * nzp;
-      for (int t = tid; t < ztasks; t += NTH) {
-        const int zb = zdiv(t, rnx), x = t - zb * nx, z0 = 8 * zb;
-        const float4 a0 = ld4(attv + x * nzp + z0), a1 = ld4(attv + x * nzp + z0 + 4);
-        const float* col = WB + x * ast;
-        float o[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) o[k] = 0.f;
-        zpassu(az, zblk, col + z0, o);
-        if (z0 == 0)
-          for (int k = 0; k < hz; ++k) o[0] = fmaf(cLz[k], col[R0 + k], o[0]);
-        if (z0 <= nz - 1 && nz - 1 < z0 + 8) {
-          const int kz = nz - 1 - z0;
-          float s = 0.f;
-          for (int k = 0; k < hz; ++k) s = fmaf(cRz[k], col[R0 + nz - 1 - k], s);
-#pragma unroll
-          for (int k = 0; k < 8; ++k)
-            if (k == kz) o[k] += s;
-        }
-        float* dst = Tp + x * nzp + z0;
-        st4(dst, make_float4(__fmul_rn(a0.x, o[0]), __fmul_rn(a0.y, o[1]), __fmul_rn(a0.z, o[2]),
-                             __fmul_rn(a0.w, o[3])));
-        st4(dst + 4, make_float4(__fmul_rn(a1.x, o[4]), __fmul_rn(a1.y, o[5]), __fmul_rn(a1.z, o[6]),
-                                 __fmul_rn(a1.w, o[7])));
+        for (int k = 0; k < W; ++k)
+          if (k == kz) o[k] += s;
       }
-      __syncthreads();
-      if (tid == 0 && qi < nitems) issue(qi, qy, b);  // this stage is free again
-      next(qi, qy);
-      b ^= 1;
+      float* dst = Tp + x * nzp + z0;
+#pragma unroll
+      for (int k = 0; k < W / 4; ++k)
+        st4(dst + 4 * k, make_float4(__fmul_rn(at[k].x, o[4 * k]), __fmul_rn(at[k].y, o[4 * k + 1]),
+                                     __fmul_rn(at[k].z, o[4 * k + 2]), __fmul_rn(at[k].w, o[4 * k + 3])));
     }
+  };
+  // prologue: the first view, the stages of p and p + 1, the x pass of p
+  load_view(i0);
+  {
+    bool ok = wait(0);
+    if (i1 < nitems) ok = wait(1) && ok;
+    if (__syncthreads_or(!ok)) {
+      give_up();
+      return;
+    }
+  }
+  xpass(stage, WB0, i0, y0);
+  __syncthreads();
+  int s = 0, w = 0;  // stage and x-pass buffer of plane p
+  for (;;) {
+    const bool h1 = i1 < nitems, h2 = i2 < nitems;
+    const int s1 = s == 2 ? 0 : s + 1;
+    const bool newv = h1 && slot_of(i1) != slot_of(i0);
+    if (newv) load_view(i1);  // the last reader of VB (the x pass of p) finished before the barrier
+    zpass(stage + s * sts, WB0 + w * wbs, i0, y0);
+    if (h1) {
+      if (newv || g.nwa == 1) __syncthreads();  // uniform
+      xpass(stage + s1 * sts, WB0 + (w ^ 1) * wbs, i1, y1);
+    }
+    bool ok = true;
+    if (h2) ok = wait(s1 == 2 ? 0 : s1 + 1);
+    if (__syncthreads_or(!ok)) {
+      give_up();
+      return;
+    }
+    if (!h1) break;
+    if (i3 < nitems) {  // stage s is free again: plane p + 3
+      if (tid == 0) issue(i3, y3, s);
+      pend |= 1u << s;
+    }
+    i0 = i1;
+    y0 = y1;
+    i1 = i2;
+    y1 = y2;
+    i2 = i3;
+    y2 = y3;
+    next(i3, y3);
+    s = s1;
+    w ^= 1;
   }
 }
 

@@ -17,6 +17,8 @@ struct ZGeom {
   int hs, ts;       // weight-row and tail-row lengths of one direction
   int rows, ast;    // z-pass buffer: rows per column, column stride (4 * odd)
   int bs;           // x-pass buffer row stride (4 * odd)
+  int nwa;          // k_zadj x-pass output buffers: 2 (double-buffered) or 1
+  int nsf;          // k_zfwd staging buffers: 2 (two planes in flight) or 1
 };
 
 __host__ __device__ constexpr int zround(int v, int m) { return (v + m - 1) / m * m; }
@@ -45,9 +47,11 @@ inline ZGeom zgeom_make(int nx, int ny, int nz, int px, int pz, int pad) {
   g.xpw = zround(g.C0 - g.hx + px, 8);
   g.hs = g.zpw + g.xpw;
   g.ts = zround(2 * g.hx + 2 * g.hz, 4) < 4 ? 4 : zround(2 * g.hx + 2 * g.hz, 4);
-  g.rows = zround(nz, 8) + g.zpw;
+  g.rows = zround(nz, 16) + g.zpw;  // z tasks of 8 or 16 outputs
   g.ast = zstride4(g.rows);
   g.bs = zstride4(nx + g.xpw);
+  g.nwa = 1;
+  g.nsf = 1;
   return g;
 }
 
@@ -57,6 +61,7 @@ struct ZArgs {
   const float* att;     // ATT
   const float* H;       // [set][y][2 hs]: fwd z | fwd x | adj z | adj x
   const float* E;       // [set][y][2 ts]: ELz ERz ELx ERx | cLx cRx cLz cRz
+  const int* R;         // [set][y][8]: (first 4-tap block, 8-tap blocks) of fwd z | fwd x | adj z | adj x
   const float4* rot;    // [view] (cos(2pi - theta), sin(2pi - theta), theta == 0, theta)
   const int* vidx;      // [nv] plan view of each slot
   const int* viewset;   // [nview] PSF set of each view
@@ -68,31 +73,36 @@ struct ZArgs {
 };
 
 // k_zfwd shared memory (floats; every region 16-byte aligned):
-//   [bar 4][stage: att plane nx*nzp | weights hs | tails ts][Hw 2 x (hs + ts)]
-//   [PA nx, PB ny (float2)][geoW nx (float4)][geoO nx (int), rounded to 4]
-//   [ZB nx * ast][XB nz * bs]
-__host__ __device__ inline size_t zfwd_smem(const ZGeom& g) {
-  const size_t f = 4 + (size_t)g.nx * g.nzp + g.hs + g.ts + 2 * (size_t)(g.hs + g.ts) + 2 * (size_t)(g.nx + g.ny) +
-                   4 * (size_t)g.nx + zround(g.nx, 4) + (size_t)g.nx * g.ast + (size_t)g.nz * g.bs;
+//   [bar 4][nsf stages: att plane nx*nzp | weights hs | tails ts][Hw 2 x (hs + ts)]
+//   [geoW nx (float4)][geoO nx (int), rounded to 4][ZB nx * ast][XB nz * bs]
+__host__ __device__ inline size_t zfwd_smem(const ZGeom& g, int nsf) {
+  const size_t f = 4 + nsf * ((size_t)g.nx * g.nzp + g.hs + g.ts) + 2 * (size_t)(g.hs + g.ts) + 4 * (size_t)g.nx +
+                   zround(g.nx, 4) + (size_t)g.nx * g.ast + (size_t)g.nz * g.bs;
   return f * sizeof(float);
 }
 
-// k_zadj shared memory (floats): [bar 4][2 stages x (weights hs | folds ts)]
-//   [VB nz * bs: the view, zero-padded, data columns C0..][WB nx * ast:
+// k_zadj shared memory (floats): [bar 8][3 stages x (weights hs | folds ts)]
+//   [VB nz * bs: the view, zero-padded, data columns C0..][nwb x WB nx * ast:
 //   x-pass output, column x, data rows R0..]
-__host__ __device__ inline size_t zadj_smem(const ZGeom& g) {
-  return sizeof(float) * (4 + 2 * (size_t)(g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)g.nx * g.ast);
+__host__ __device__ inline size_t zadj_smem(const ZGeom& g, int nwb) {
+  return sizeof(float) *
+         (8 + 3 * (size_t)(g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)nwb * g.nx * g.ast);
 }
 
-// launch shapes of k_zfwd / k_zadj: NT tasks per thread, NTH threads
+// launch shapes of k_zfwd / k_zadj: NT tasks of W outputs per thread, NTH
+// threads (W = 16 needs nx % 16 == 0); fwd: the forward compiles without
+// register spills in this shape (with the accumulators, 1024 threads and the
+// largest NT leave too few registers)
 struct ZShape {
-  int nt, nth;
+  int nt, nth, w, fwd;
 };
-constexpr int kZNShapes = 8;
-constexpr ZShape kZShapes[kZNShapes] = {{1, 512}, {2, 512}, {3, 512}, {4, 512}, {1, 640}, {2, 640}, {3, 640}, {1, 1024}};
-// forward shapes that compile without register spills: not 1024 threads
-// (with the accumulators they leave too few registers)
-inline bool zfwd_shape_ok(int i) { return kZShapes[i].nth <= 640; }
+constexpr int kZNShapes = 13;
+constexpr ZShape kZShapes[kZNShapes] = {{1, 512, 8, 1},  {2, 512, 8, 1},  {3, 512, 8, 1},   {4, 512, 8, 1},
+                                        {1, 640, 8, 1},  {2, 640, 8, 1},  {3, 640, 8, 0},   {1, 1024, 8, 0},
+                                        {1, 512, 16, 1}, {2, 512, 16, 1}, {1, 640, 16, 1},  {2, 640, 16, 0},
+                                        {1, 1024, 16, 0}};
+inline bool zfwd_shape_ok(int i) { return kZShapes[i].fwd != 0; }
+inline bool zshape_fits(const ZGeom& g, int i) { return g.nx % kZShapes[i].w == 0; }
 
 // launchers (zpath_inst.cu)
 cudaError_t zpath_setup(int max_smem);

@@ -5,9 +5,13 @@
 namespace spect {
 
 namespace {
+// the order of kZShapes
 #define ZSHAPES(K)                                                                                           \
-  {(const void*)K<1, 512>, (const void*)K<2, 512>, (const void*)K<3, 512>, (const void*)K<4, 512>,        \
-   (const void*)K<1, 640>, (const void*)K<2, 640>, (const void*)K<3, 640>, (const void*)K<1, 1024>}
+  {(const void*)K<1, 512, 8>,  (const void*)K<2, 512, 8>,   (const void*)K<3, 512, 8>,                       \
+   (const void*)K<4, 512, 8>,  (const void*)K<1, 640, 8>,   (const void*)K<2, 640, 8>,                       \
+   (const void*)K<3, 640, 8>,  (const void*)K<1, 1024, 8>,  (const void*)K<1, 512, 16>,                      \
+   (const void*)K<2, 512, 16>, (const void*)K<1, 640, 16>,  (const void*)K<2, 640, 16>,                      \
+   (const void*)K<1, 1024, 16>}
 const void* const kZfwd[kZNShapes] = ZSHAPES(k_zfwd);
 const void* const kZadj[kZNShapes] = ZSHAPES(k_zadj);
 #undef ZSHAPES

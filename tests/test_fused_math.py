@@ -41,7 +41,7 @@ def zgeom(nx, nz, px, pz):
     g["xpw"] = zround(g["C0"] - g["hx"] + px, 8)
     g["hs"] = g["zpw"] + g["xpw"]
     g["ts"] = max(4, zround(2 * g["hx"] + 2 * g["hz"], 4))
-    g["rows"] = zround(nz, 8) + g["zpw"]
+    g["rows"] = zround(nz, 16) + g["zpw"]
     g["ast"] = zstride4(g["rows"])
     g["bs"] = zstride4(nx + g["xpw"])
     return g
@@ -199,15 +199,21 @@ def test_gather_candidates_cover_the_forward_footprints(nx, nview):
 def test_fused_buffer_bounds(nx, nz, px, pz):
     """Every index the fused kernels form stays inside its buffer."""
     g = zgeom(nx, nz, px, pz)
-    nzb, nz4 = (nz + 7) // 8, (nz + 3) // 4
+    nz4 = (nz + 3) // 4
     assert g["ast"] % 4 == 0 and (g["ast"] // 4) % 2 == 1 and g["bs"] % 4 == 0 and (g["bs"] // 4) % 2 == 1
     assert g["hs"] % 8 == 0 and g["ts"] % 4 == 0 and g["nzp"] % 16 == 0
-    # z-pass buffer: build stores rows R0 + 4 zg + 3; windows read rows z0 .. z0 + zpw + 7
+    # z-pass buffer: build stores rows R0 + 4 zg + 3
     assert g["R0"] + 4 * nz4 <= g["ast"]
-    assert 8 * (nzb - 1) + g["zpw"] + 8 <= g["rows"] <= g["ast"]
     assert g["R0"] + nz <= g["ast"]  # adjoint x-pass stores and edge reads
-    # x-pass buffer: z-pass stores column C0 + nx - 1; windows read x0 .. x0 + xpw + 7
-    assert g["C0"] + nx <= g["bs"] and (nx - 8) + g["xpw"] + 8 <= g["bs"]
+    for W in (8, 16):  # task widths; W = 16 only where W divides nx
+        nzb = (nz + W - 1) // W
+        # windows read rows z0 .. z0 + zpw + W - 1; adjoint z-pass stores z0 .. z0 + W - 1 of a T column
+        assert W * (nzb - 1) + g["zpw"] + W <= g["rows"] <= g["ast"]
+        assert W * nzb <= g["nzp"]
+        if nx % W:
+            continue
+        # x-pass buffer: z-pass stores column C0 + nx - 1; windows read x0 .. x0 + xpw + W - 1
+        assert g["C0"] + nx <= g["bs"] and (nx - W) + g["xpw"] + W <= g["bs"]
     # tap shift inside the window
     assert g["R0"] - g["hz"] + pz <= g["zpw"] and g["C0"] - g["hx"] + px <= g["xpw"]
     # IZ: the farthest tap of the farthest in-grid sample, plus the z group
@@ -220,3 +226,63 @@ def test_fused_buffer_bounds(nx, nz, px, pz):
     assert np.floor((nx - 1) / 2 - r) >= -g["pad"] and np.floor((nx - 1) / 2 + r) <= jmax
     # the adjoint planes' z blocks end inside the padded column
     assert 8 * nzb <= nzp
+
+
+def trim_taps(w):
+    """Mirror of trim_taps (csrc/spect_gpu.cu): zero the outer taps while their
+    summed magnitude per side stays within 2^-27 of the factor's."""
+    w = np.array(w, np.float64)
+    lim = np.ldexp(np.abs(w).sum(), -27)
+    acc = 0.0
+    for i in range(len(w)):
+        acc += abs(w[i])
+        if acc > lim:
+            break
+        w[i] = 0.0
+    acc = 0.0
+    for i in range(len(w) - 1, -1, -1):
+        acc += abs(w[i])
+        if acc > lim:
+            break
+        w[i] = 0.0
+    return w
+
+
+def tap_range(row):
+    """Mirror of tap_range: (first 4-tap block, 8-tap blocks) covering the
+    nonzero taps of a pass row, within the row."""
+    nzi = np.flatnonzero(row)
+    lo, hi = nzi[0], nzi[-1]
+    b = lo // 4
+    n = (hi + 1 - 4 * b + 7) // 8
+    if 4 * b + 8 * n > len(row):
+        b -= 1
+    return b, n
+
+
+@pytest.mark.parametrize("nx,nz,p,f0,f1", [(128, 80, 37, 1.0, 6.0), (64, 64, 11, 1.0, 3.0), (256, 200, 65, 1.0, 6.0),
+                                          (96, 48, 21, 0.5, 8.0), (40, 37, 9, 1.0, 2.5)])
+def test_trimmed_taps_and_ranges(nx, nz, p, f0, f1):
+    """Trimmed factors leave out at most 2^-26 of a factor's mass; each pass's
+    tap-block range covers every kept tap and stays inside its row; the
+    trimmed clamped convolution equals the full one to 2^-24 relative."""
+    from oracle import oracle as O
+    g = zgeom(nx, nz, p, p)
+    psf = O.psf_gauss(nx, p, p, f0, f1, None, None, None, np.float64)
+    h = (p - 1) // 2
+    rng = np.random.default_rng(p)
+    line = rng.random(nz)
+    for y in range(0, nx, max(1, nx // 16)):
+        a = psf[:, h, y] / psf[h, h, y]
+        t = trim_taps(a)
+        assert np.abs(a - t).sum() <= 2.0 ** -26 * np.abs(a).sum()
+        assert t[h] == a[h]
+        s = g["R0"] - g["hz"]
+        row = np.zeros(g["zpw"])
+        row[s:s + p] = t[::-1]
+        b4, n8 = tap_range(row)
+        assert b4 >= 0 and n8 >= 1 and 4 * b4 + 8 * n8 <= g["zpw"]
+        nzi = np.flatnonzero(row)
+        assert 4 * b4 <= nzi[0] and nzi[-1] < 4 * b4 + 8 * n8
+        full, cut = clamp_conv(line, a[::-1]), clamp_conv(line, t[::-1])
+        assert np.abs(full - cut).max() <= 2.0 ** -24 * np.abs(full).max()

@@ -90,3 +90,77 @@ def test_config_parity_one(S, O):
     rng = np.random.default_rng(3)
     y = np.asfortranarray(rng.random((128, 80, len(idx))), np.float32)
     assert relerr(S.backproject(y, plan, index=idx), G.backproject(y, index=idx)) <= TOL
+
+
+@pytest.mark.parametrize("nbuf,zw,stages", [("1", "8", "1"), ("2", "8", "2"), ("1", "16", "2"), ("2", "16", "1")])
+def test_fused_pair_plane_walk(S, O, monkeypatch, nbuf, zw, stages):
+    """Fused pair walking several work items per block (60 views of 64x64x40:
+    more (view, depth chunk) items than SMs), convolution tasks of 8 and of 16
+    outputs, the adjoint x pass with one and with two buffers, the forward
+    with one and with two staging buffers; all views, a subset, and one OS-EM
+    iteration."""
+    monkeypatch.setenv("SPECT_ZADJ_BUFFERS", nbuf)
+    monkeypatch.setenv("SPECT_ZW", zw)
+    monkeypatch.setenv("SPECT_ZFWD_STAGES", stages)
+    st = _study(S, 64, 40, 60, 11, 3.0, (0.0096, 0.015), seed=5)
+    plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    assert plan.fused
+    G = O.Geometry(st.mumap, st.psfs, st.dy)
+    assert relerr(S.project(st.image, plan), G.project(st.image)) <= TOL
+    rng = np.random.default_rng(4)
+    y = np.asfortranarray(rng.random((64, 40, 60)), np.float32)
+    assert relerr(S.backproject(y, plan), G.backproject(y)) <= TOL
+    idx = np.array([1, 13, 44], np.int32)
+    ys = np.asfortranarray(y[:, :, idx])
+    assert relerr(S.backproject(ys, plan, index=idx), G.backproject(ys, index=idx)) <= TOL
+    x0 = np.ones(st.image.shape, np.float32, order="F")
+    yn = np.asfortranarray(np.maximum(G.project(st.image), 0) + 1, np.float32)
+    bg = np.full(yn.shape, 1.0, np.float32, order="F")
+    assert relerr(S.osem(x0, yn, bg, S.Ablock(plan, 4), niter=1), G.osem(x0, yn, bg, 4, 1)) <= TOL
+
+
+def test_fused_pair_odd_width(S, O):
+    """Fused pair with nx = 40 (a multiple of 8, not of 16: 8-output tasks)
+    and nz = 37 (a partial last z task)."""
+    st = _study(S, 40, 37, 24, 9, 2.5, (0.0096, 0.015), seed=11)
+    plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    assert plan.fused
+    G = O.Geometry(st.mumap, st.psfs, st.dy)
+    assert relerr(S.project(st.image, plan), G.project(st.image)) <= TOL
+    rng = np.random.default_rng(6)
+    y = np.asfortranarray(rng.random((40, 37, 24)), np.float32)
+    assert relerr(S.backproject(y, plan), G.backproject(y)) <= TOL
+
+
+def test_trimmed_taps_match_full(S, O, monkeypatch):
+    """Skipping the outer PSF taps below Float32 resolution (the default)
+    against every tap (SPECT_ZTRIM=0): the same projections and
+    back-projections to 1e-6, both within the oracle tolerance."""
+    st = _study(S, 128, 80, 120, 37, 6.0, (0.0096, 0.015), seed=21)
+    idx = np.array([0, 7, 30, 61, 119], np.int32)
+    rng = np.random.default_rng(8)
+    y = np.asfortranarray(rng.random((128, 80, len(idx))), np.float32)
+    out = {}
+    for trim in ("1", "0"):
+        monkeypatch.setenv("SPECT_ZTRIM", trim)
+        plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+        assert plan.fused
+        out[trim] = (S.project(st.image, plan, index=idx), S.backproject(y, plan, index=idx))
+    G = O.Geometry(st.mumap, st.psfs, st.dy)
+    v_ref, b_ref = G.project(st.image, index=idx), G.backproject(y, index=idx)
+    for trim in ("1", "0"):
+        assert relerr(out[trim][0], v_ref) <= TOL
+        assert relerr(out[trim][1], b_ref) <= TOL
+    assert relerr(out["1"][0], out["0"][0]) <= 1e-6
+    assert relerr(out["1"][1], out["0"][1]) <= 1e-6
+
+
+def test_wide_psf_takes_split_path(S, O):
+    """A PSF row longer than the fused passes' 9 blocks of 8 taps (75 taps)
+    runs the split kernels, with the same results as the oracle."""
+    st = _study(S, 64, 24, 12, 75, 6.0, (0.0096, 0.015), seed=31)
+    plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    assert not plan.fused
+    G = O.Geometry(st.mumap, st.psfs, st.dy)
+    idx = np.array([0, 5], np.int32)
+    assert relerr(S.project(st.image, plan, index=idx), G.project(st.image, index=idx)) <= TOL
