@@ -166,41 +166,46 @@ def peaks(S, L):
 
 
 def launch_work(plan, kind, nv):
-    """(kernel name, bound, algorithmic FLOPs, algorithmic bytes) of one launch
-    of kernel kind `kind` processing nv views, for the path the plan runs.
-    FLOPs count the convolution taps (1 FMA = 2 FLOP per tap of the z and x
-    passes) plus the bilinear sample and attenuation; bytes count each
-    compulsory array once (attenuation planes, adjoint planes, images).  The
-    fused pair counts the taps it keeps per plane (the outer taps below
-    Float32 resolution of a plane's factors are skipped), so its fraction
-    measures the arithmetic it does, not the full-width work it avoids."""
+    """(kernel name, bound, algorithmic FLOPs, algorithmic bytes, executed
+    FLOPs or None) of one launch of kernel kind `kind` processing nv views,
+    for the path the plan runs.  The algorithmic FLOPs of a convolution
+    kernel are the fixed per-pass formula of the reference's algorithm (two
+    real 2-D FFTs and a spectrum multiply per plane at its padded sizes,
+    fft_flops), whatever this kernel does instead; the executed FLOPs are the
+    FMAs it runs (1 FMA = 2 FLOP per kept tap of the z and x passes, plus the
+    bilinear sample and attenuation).  The fused pair skips the outer taps
+    below Float32 resolution of each plane's factors, so it counts the kept
+    taps.  Bytes count each compulsory array once (attenuation planes,
+    adjoint planes, images)."""
     nx, ny, nz = plan.imgsize
     px, pz = plan.px, plan.pz
     N, nxz = nx * ny * nz, nx * nz
     nzp = 16 * ((nz + 15) // 16)
+    Npx = 1 << int(np.ceil(np.log2(nx + px - 1)))
+    Npz = 1 << int(np.ceil(np.log2(nz + pz - 1)))
+    F = fft_flops(nv, ny, Npx, Npz)
     if plan.fused:
         tz, tx = plan.conv_taps()
         table = {
-            "k_conv_fwd": ("k_zfwd", "fp32", nv * ny * nx * nz * (2.0 * (tx + tz) + 8), 4.0 * (nv * ny * nx * nzp + N)),
-            "k_conv_adj": ("k_zadj", "fp32", nv * ny * nx * nz * (2.0 * (tx + tz) + 1), 4.0 * (2 * nv * ny * nx * nzp + nv * nxz)),
-            "k_rot_adj": ("k_zrot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * ny * nx * nzp + 3 * N)),
-            "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz),
-            "k_reduce_image": ("k_from_iz", "hbm", 0.0, 4.0 * 2 * N),
+            "k_conv_fwd": ("k_zfwd", "fp32", F, 4.0 * (nv * ny * nx * nzp + N), nv * ny * nx * nz * (2.0 * (tx + tz) + 8)),
+            "k_conv_adj": ("k_zadj", "fp32", F, 4.0 * (2 * nv * ny * nx * nzp + nv * nxz),
+                           nv * ny * nx * nz * (2.0 * (tx + tz) + 1)),
+            "k_rot_adj": ("k_zrot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * ny * nx * nzp + 3 * N), None),
+            "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz, None),
+            "k_reduce_image": ("k_from_iz", "hbm", 0.0, 4.0 * 2 * N, None),
         }
     else:
         conv = plan.conv_kernels()
-        Npx = 1 << int(np.ceil(np.log2(nx + px - 1)))
-        Npz = 1 << int(np.ceil(np.log2(nz + pz - 1)))
-        cf = {"direct": direct_flops(nv, ny, nx, nz, px, pz), "fft": fft_flops(nv, ny, Npx, Npz)}
+        ex = {"direct": direct_flops(nv, ny, nx, nz, px, pz), "fft": None}
         table = {
-            "k_rot_fwd": ("k_rot_fwd", "hbm", 8.0 * nv * N, 4.0 * (N + nv * N)),
+            "k_rot_fwd": ("k_rot_fwd", "hbm", 8.0 * nv * N, 4.0 * (N + nv * N), None),
             "k_conv_fwd": ("k_sconv_fwd" if conv["forward"] == "direct" else "k_conv_fwd2", "fp32",
-                           cf[conv["forward"]], 4.0 * (2 * nv * N)),
+                           F, 4.0 * (2 * nv * N), ex[conv["forward"]]),
             "k_conv_adj": ("k_sconv_adj" if conv["adjoint"] == "direct" else "k_conv_adj2", "fp32",
-                           cf[conv["adjoint"]], 4.0 * (2 * nv * N)),
-            "k_rot_adj": ("k_rot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * N + N)),
-            "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz),
-            "k_reduce_image": ("k_reduce_image", "hbm", 0.0, 4.0 * 3 * N),
+                           F, 4.0 * (2 * nv * N), ex[conv["adjoint"]]),
+            "k_rot_adj": ("k_rot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * N + N), None),
+            "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz, None),
+            "k_reduce_image": ("k_reduce_image", "hbm", 0.0, 4.0 * 3 * N, None),
         }
     return table.get(kind)
 
@@ -220,12 +225,16 @@ def kernel_table(plan, kms, kn, steps, nv, pk, min_share=0.10):
                "launches_per_step": int(kn[k] // steps), "share": round(ms / total, 3),
                "avg_launch_ms": round(avg, 4)}
         if w:
-            name, bound, flops, nbytes = w
+            name, bound, flops, nbytes, xflops = w
             tf = flops / (avg / 1e3) / 1e12
             gbs = nbytes / (avg / 1e3) / 1e9
             if bound == "fp32":
                 row.update(bound="fp32", achieved=round(tf, 3), peak=pk["fp32_tflops"], unit="TFLOP/s",
                            frac=round(tf / pk["fp32_tflops"], 4))
+                if xflops is not None:
+                    xt = xflops / (avg / 1e3) / 1e12
+                    row.update(executed_flops_per_launch=xflops, executed_tflops=round(xt, 3),
+                               executed_frac=round(xt / pk["fp32_tflops"], 4))
             else:
                 row.update(bound="hbm", achieved=round(gbs, 1), peak=pk["hbm_gbs"], unit="GB/s",
                            frac=round(gbs / pk["hbm_gbs"], 4))

@@ -104,15 +104,22 @@ __device__ __forceinline__ void zpassw(const float* __restrict__ w, int b4, int 
   }
 }
 
-// sum_{k < n} c[k] v[step k] for n <= 36 (a half width of a row of at most
-// 72 taps): predicated and fully unrolled, so every load is issued at once,
-// into four partial sums over k mod 4 added as (s0 + s1) + (s2 + s3)
+// sum_{k < n} c[k] v[step k]: four partial sums over k mod 4, added as
+// (s0 + s1) + (s2 + s3); four taps' loads per round are independent, so a
+// round waits for one load latency
 __device__ __forceinline__ float zfold(const float* c, const float* v, int step, int n) {
-  float s[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-  for (int k = 0; k < 36; ++k)
-    if (k < n) s[k & 3] = fmaf(c[k], v[step * k], s[k & 3]);
-  return (s[0] + s[1]) + (s[2] + s[3]);
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    s0 = fmaf(c[k], v[step * k], s0);
+    s1 = fmaf(c[k + 1], v[step * (k + 1)], s1);
+    s2 = fmaf(c[k + 2], v[step * (k + 2)], s2);
+    s3 = fmaf(c[k + 3], v[step * (k + 3)], s3);
+  }
+  if (k < n) s0 = fmaf(c[k], v[step * k], s0);
+  if (k + 1 < n) s1 = fmaf(c[k + 1], v[step * (k + 1)], s1);
+  if (k + 2 < n) s2 = fmaf(c[k + 2], v[step * (k + 2)], s2);
+  return (s0 + s1) + (s2 + s3);
 }
 
 // q = t / n for 0 <= t < 2^20, 1 <= n <= 4096, with r = 1/n rounded to float:
@@ -265,10 +272,11 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts, nsf = g.nsf;
   float* const base = reinterpret_cast<float*>(smem4);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);  // nsf barriers
-  const int sts = nx * nzp + hs + ts;  // stage: attenuation plane [x][nzp], weights, tails
+  const int hts = hs + ts + 4;         // weights, tails, tap ranges of one plane (4 ints)
+  const int sts = nx * nzp + hts;      // stage: attenuation plane [x][nzp], then those
   float* const stage = base + 4;
-  float* const Hw0 = stage + nsf * sts;           // working weights, two planes
-  float4* const geoW = reinterpret_cast<float4*>(Hw0 + 2 * (hs + ts));
+  float* const Hw0 = stage + nsf * sts;           // working weights, tails, ranges: two planes
+  float4* const geoW = reinterpret_cast<float4*>(Hw0 + 2 * hts);
   int* const geoO = reinterpret_cast<int*>(geoW + nx);
   float* const ZB = reinterpret_cast<float*>(geoO + zround(nx, 4));  // [x][ast], data rows R0..R0+nz-1
   float* const XB = ZB + (size_t)nx * g.ast;                          // [z][bs], data columns C0..C0+nx-1
@@ -283,10 +291,11 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
     float* sA = stage + s * sts;
     float* sW = sA + nx * nzp;
     fence_proxy_async();
-    mbar_expect(&bar[s], abytes + (unsigned)((hs + ts) * sizeof(float)));
+    mbar_expect(&bar[s], abytes + (unsigned)(hts * sizeof(float)));
     bulk_copy(&bar[s], sA, a.att + ((size_t)v * ny + y) * nx * nzp, abytes);
     bulk_copy(&bar[s], sW, a.H + ((size_t)set * ny + y) * (2 * hs), (unsigned)(hs * sizeof(float)));
     bulk_copy(&bar[s], sW + hs, a.E + ((size_t)set * ny + y) * (2 * ts), (unsigned)(ts * sizeof(float)));
+    bulk_copy(&bar[s], sW + hs + ts, a.R + ((size_t)set * ny + y) * 8, 4u * sizeof(int));
   };
   auto next = [&](int& item, int& y) {
     const int yend = min(ny, chunk_of(item) * a.chunkY + a.chunkY);
@@ -373,20 +382,36 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
   auto gather = [&](int s, int hb) {
     const float* const sA = stage + s * sts;
     const float* const sW = sA + nx * nzp;
-    float* const Hw = Hw0 + hb * (hs + ts);
+    float* const Hw = Hw0 + hb * hts;
     for (int k = tid; k < hs + ts; k += NTH) Hw[k] = sW[k];
-    for (int u = tid; u < units; u += NTH) {
-      const int x = zdiv(u, rnz4), zg = u - x * nz4;
-      const float4 w = geoW[x];
-      const float* p = a.img + geoO[x] + 4 * zg;
-      const float4 t0 = ld4(p), t1 = ld4(p + nzp), t2 = ld4(p + Lz), t3 = ld4(p + Lz + nzp);
-      const float4 at = ld4(sA + x * nzp + 4 * zg);
-      float4 o;
-      o.x = __fmul_rn(fmaf(w.w, t3.x, fmaf(w.z, t2.x, fmaf(w.y, t1.x, __fmul_rn(w.x, t0.x)))), at.x);
-      o.y = __fmul_rn(fmaf(w.w, t3.y, fmaf(w.z, t2.y, fmaf(w.y, t1.y, __fmul_rn(w.x, t0.y)))), at.y);
-      o.z = __fmul_rn(fmaf(w.w, t3.z, fmaf(w.z, t2.z, fmaf(w.y, t1.z, __fmul_rn(w.x, t0.z)))), at.z);
-      o.w = __fmul_rn(fmaf(w.w, t3.w, fmaf(w.z, t2.w, fmaf(w.y, t1.w, __fmul_rn(w.x, t0.w)))), at.w);
-      st4(ZB + x * ast + R0 + 4 * zg, o);
+    if (tid < 4) reinterpret_cast<int*>(Hw + hs + ts)[tid] = reinterpret_cast<const int*>(sW + hs + ts)[tid];
+    // two units per round, both units' image loads issued before either is used
+    for (int u0 = tid; u0 < units; u0 += 2 * NTH) {
+      float4 t[2][4];
+      int xs[2], zs[2];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int u = min(u0 + j * NTH, units - 1);  // a repeated last unit stores the same values
+        xs[j] = zdiv(u, rnz4);
+        zs[j] = u - xs[j] * nz4;
+        const float* p = a.img + geoO[xs[j]] + 4 * zs[j];
+        t[j][0] = ld4(p);
+        t[j][1] = ld4(p + nzp);
+        t[j][2] = ld4(p + Lz);
+        t[j][3] = ld4(p + Lz + nzp);
+      }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const float4 w = geoW[xs[j]];
+        const float4 at = ld4(sA + xs[j] * nzp + 4 * zs[j]);
+        const float4 t0 = t[j][0], t1 = t[j][1], t2 = t[j][2], t3 = t[j][3];
+        float4 o;
+        o.x = __fmul_rn(fmaf(w.w, t3.x, fmaf(w.z, t2.x, fmaf(w.y, t1.x, __fmul_rn(w.x, t0.x)))), at.x);
+        o.y = __fmul_rn(fmaf(w.w, t3.y, fmaf(w.z, t2.y, fmaf(w.y, t1.y, __fmul_rn(w.x, t0.y)))), at.y);
+        o.z = __fmul_rn(fmaf(w.w, t3.z, fmaf(w.z, t2.z, fmaf(w.y, t1.z, __fmul_rn(w.x, t0.z)))), at.z);
+        o.w = __fmul_rn(fmaf(w.w, t3.w, fmaf(w.z, t2.w, fmaf(w.y, t1.w, __fmul_rn(w.x, t0.w)))), at.w);
+        st4(ZB + xs[j] * ast + R0 + 4 * zs[j], o);
+      }
     }
   };
   float acc[NT][W];
@@ -411,8 +436,8 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
   int hb = 0, s1 = nsf > 1 ? 1 : 0;  // working-weight buffer of plane p, stage of plane p + 1
   for (;;) {
     const bool h1 = i1 < nitems;
-    const float* Hw = Hw0 + hb * (hs + ts);
-    const int4 rg = *reinterpret_cast<const int4*>(a.R + ((size_t)a.viewset[a.vidx[slot_of(i0)]] * ny + y0) * 8);
+    const float* Hw = Hw0 + hb * hts;
+    const int4 rg = *reinterpret_cast<const int4*>(Hw + hs + ts);  // tap ranges: z pass, x pass
     // phase A: z pass of p, task (x, z block) -> XB rows z, column C0 + x
     const float* ELz = Hw + hs;
     const float* ERz = ELz + hz;
@@ -520,7 +545,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts;
   float* const base = reinterpret_cast<float*>(smem4);
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(base);  // three barriers
-  const int sts = hs + ts;                 // one stage: weights, folds
+  const int sts = hs + ts + 4;             // one stage: weights, folds, tap ranges (4 ints)
   float* const stage = base + 8;
   float* const VB = stage + 3 * sts;
   float* const WB0 = VB + (size_t)nz * g.bs;
@@ -534,9 +559,10 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
     const int sl = slot_of(item), v = a.vidx[sl], set = a.viewset[v];
     float* st = stage + s * sts;
     fence_proxy_async();
-    mbar_expect(&bar[s], (unsigned)((hs + ts) * sizeof(float)));
+    mbar_expect(&bar[s], (unsigned)(sts * sizeof(float)));
     bulk_copy(&bar[s], st, a.H + ((size_t)set * ny + y) * (2 * hs) + hs, (unsigned)(hs * sizeof(float)));
     bulk_copy(&bar[s], st + hs, a.E + ((size_t)set * ny + y) * (2 * ts) + ts, (unsigned)(ts * sizeof(float)));
+    bulk_copy(&bar[s], st + hs + ts, a.R + ((size_t)set * ny + y) * 8 + 4, 4u * sizeof(int));
   };
   auto next = [&](int& item, int& y) {
     const int yend = min(ny, chunk_of(item) * a.chunkY + a.chunkY);
@@ -589,16 +615,26 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   const int nzb = (nz + W - 1) / W, ztasks = nx * nzb, xtasks = nz * (nx / W);
   const int ast = g.ast, bs = g.bs, R0 = g.R0, C0 = g.C0, hz = g.hz, hx = g.hx;
   const float rnx = 1.0f / nx, rnz = 1.0f / nz;
-  auto load_view = [&](int item) {  // the item's view, zero-padded
+  // the item's view into VB, zero-padded: element e = z bs + c, eight per
+  // thread and round with all eight loads issued before the stores
+  const float rbs = 1.0f / bs;
+  auto load_view = [&](int item) {
     const float* V = a.views + (size_t)slot_of(item) * nz * nx;
-    for (int z = tid / 32; z < nz; z += NTH / 32) {
-      float* row = VB + (size_t)z * bs;
-      for (int c = tid & 31; c < bs; c += 32) row[c] = (c >= C0 && c < C0 + nx) ? V[z * nx + c - C0] : 0.f;
+    for (int e0 = tid; e0 < nz * bs; e0 += 8 * NTH) {
+      float v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int e = e0 + j * NTH, z = zdiv(e, rbs), c = e - z * bs;
+        v[j] = (e < nz * bs && c >= C0 && c < C0 + nx) ? V[z * nx + c - C0] : 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (e0 + j * NTH < nz * bs) VB[e0 + j * NTH] = v[j];
     }
   };
   // x pass of the plane whose stage is st: task (z, x block) -> WB column x, row R0 + z
   auto xpass = [&](const float* st, float* WB, int item, int y) {
-    const int2 rg = *reinterpret_cast<const int2*>(a.R + ((size_t)a.viewset[a.vidx[slot_of(item)]] * ny + y) * 8 + 6);
+    const int2 rg = *reinterpret_cast<const int2*>(st + hs + ts + 2);  // x-pass tap range
     const float* ax = st + g.zpw;     // adjoint x weights (shifted)
     const float* cLx = st + hs;       // folds
     const float* cRx = cLx + hx;
@@ -623,7 +659,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
   // z pass of plane (item, y), stage st: task (x, z block) -> T column (x, y) of the slot
   auto zpass = [&](const float* st, const float* WB, int item, int y) {
     const int slot = slot_of(item), v = a.vidx[slot];
-    const int2 rg = *reinterpret_cast<const int2*>(a.R + ((size_t)a.viewset[v] * ny + y) * 8 + 4);
+    const int2 rg = *reinterpret_cast<const int2*>(st + hs + ts);  // z-pass tap range
     const float* az = st;             // adjoint z weights (shifted)
     const float* cLz = st + hs + 2 * hx;
     const float* cRz = cLz + hz;
@@ -703,9 +739,9 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 
 // ------------------------------------------------------------------------
 // k_zrot_adj<ZPL>: two 8-lane groups of a warp own image column p = (j1, j2)
-// (grid-stride), lane l of a group the z values l + 8 q, q < ZPL (nzp =
-// 8 ZPL): one 32-byte sector per group and load, the candidate geometry shared
-// by the group's 8 lanes.  The first group sums the even slots, the second
+// (grid-stride), lane l of a group the z pairs 2 l + 16 q, q < ZPL / 2 (nzp =
+// 8 ZPL): 64 contiguous bytes per group and 8-byte load, the candidate
+// geometry shared by the group's 8 lanes.  The first group sums the even slots, the second
 // the odd ones; a shuffle adds the two partial sums (a fixed order).  For
 // every slot, the rotated-grid points (x, y) whose bilinear footprint contains
 // (j1, j2) -- those with floor(s1) in {j1-1, j1} and floor(s2) in {j2-1, j2}
@@ -729,9 +765,9 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
     const bool own = p0 + ((threadIdx.x >> 4) & 1) < nx * nx;
     const int j2 = p / nx, j1 = p - j2 * nx;
     const float fj1 = (float)j1, fj2 = (float)j2;
-    float acc[ZPL];
+    float2 acc[ZPL / 2];
 #pragma unroll
-    for (int q = 0; q < ZPL; ++q) acc[q] = 0.f;
+    for (int q = 0; q < ZPL / 2; ++q) acc[q] = make_float2(0.f, 0.f);
     for (int s = half; s < nv; s += 2) {
       const float4 r = rot[vidx[s]];
       const float cs = r.x, sn = r.y;
@@ -740,7 +776,7 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
       const float rr = fabsf(cs) + fabsf(sn) + 0.01f;
       const int xlo = max(0, (int)ceilf(xc - rr)), xhi = min(nx - 1, (int)floorf(xc + rr));
       const int ylo = max(0, (int)ceilf(yc - rr)), yhi = min(ny - 1, (int)floorf(yc + rr));
-      const float* Ts = T + (size_t)s * ny * nx * nzp + lane;
+      const float* Ts = T + (size_t)s * ny * nx * nzp + 2 * lane;
       // the candidates first (weights, column offsets; 0 for the invalid
       // ones), then their loads, so that a group has all of them in flight
       float cw[9];
@@ -771,21 +807,33 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
         if (co[c] >= 0) {
           const float* tp = Ts + co[c];
 #pragma unroll
-          for (int q = 0; q < ZPL; ++q) acc[q] = fmaf(cw[c], tp[8 * q], acc[q]);
+          for (int q = 0; q < ZPL / 2; ++q) {
+            const float2 t = *reinterpret_cast<const float2*>(tp + 16 * q);
+            acc[q].x = fmaf(cw[c], t.x, acc[q].x);
+            acc[q].y = fmaf(cw[c], t.y, acc[q].y);
+          }
         }
     }
 #pragma unroll
-    for (int q = 0; q < ZPL; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], 8);  // even + odd slots
+    for (int q = 0; q < ZPL / 2; ++q) {  // even + odd slots
+      acc[q].x += __shfl_xor_sync(0xffffffffu, acc[q].x, 8);
+      acc[q].y += __shfl_xor_sync(0xffffffffu, acc[q].y, 8);
+    }
     if (half || !own) continue;
-    const size_t o = ((size_t)(j2 + g.pad) * g.L + j1 + g.pad) * nzp + lane;
+    const size_t o = ((size_t)(j2 + g.pad) * g.L + j1 + g.pad) * nzp + 2 * lane;
 #pragma unroll
-    for (int q = 0; q < ZPL; ++q) {
-      if (lane + 8 * q < g.nz) {
-        float v = acc[q];
-        if (prev) v += prev[o + 8 * q];
-        if (mode == 1 && v == 0.f) v = __int_as_float(0x7f800000);
-        if (mode == 2) v = x[o + 8 * q] * (v / asum[o + 8 * q]);
-        out[o + 8 * q] = v;
+    for (int q = 0; q < ZPL / 2; ++q) {
+      const float vq[2] = {acc[q].x, acc[q].y};
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const size_t oe = o + 16 * q + e;
+        if (2 * lane + 16 * q + e < g.nz) {
+          float v = vq[e];
+          if (prev) v += prev[oe];
+          if (mode == 1 && v == 0.f) v = __int_as_float(0x7f800000);
+          if (mode == 2) v = x[oe] * (v / asum[oe]);
+          out[oe] = v;
+        }
       }
     }
   }

@@ -73,20 +73,21 @@ struct ZArgs {
 };
 
 // k_zfwd shared memory (floats; every region 16-byte aligned):
-//   [bar 4][nsf stages: att plane nx*nzp | weights hs | tails ts][Hw 2 x (hs + ts)]
-//   [geoW nx (float4)][geoO nx (int), rounded to 4][ZB nx * ast][XB nz * bs]
+//   [bar 4][nsf stages: att plane nx*nzp | weights hs | tails ts | ranges 4]
+//   [Hw 2 x (hs + ts + 4)][geoW nx (float4)][geoO nx (int), rounded to 4]
+//   [ZB nx * ast][XB nz * bs]
 __host__ __device__ inline size_t zfwd_smem(const ZGeom& g, int nsf) {
-  const size_t f = 4 + nsf * ((size_t)g.nx * g.nzp + g.hs + g.ts) + 2 * (size_t)(g.hs + g.ts) + 4 * (size_t)g.nx +
-                   zround(g.nx, 4) + (size_t)g.nx * g.ast + (size_t)g.nz * g.bs;
+  const size_t f = 4 + nsf * ((size_t)g.nx * g.nzp + g.hs + g.ts + 4) + 2 * (size_t)(g.hs + g.ts + 4) +
+                   4 * (size_t)g.nx + zround(g.nx, 4) + (size_t)g.nx * g.ast + (size_t)g.nz * g.bs;
   return f * sizeof(float);
 }
 
-// k_zadj shared memory (floats): [bar 8][3 stages x (weights hs | folds ts)]
+// k_zadj shared memory (floats): [bar 8][3 stages x (weights hs | folds ts | ranges 4)]
 //   [VB nz * bs: the view, zero-padded, data columns C0..][nwb x WB nx * ast:
 //   x-pass output, column x, data rows R0..]
 __host__ __device__ inline size_t zadj_smem(const ZGeom& g, int nwb) {
   return sizeof(float) *
-         (8 + 3 * (size_t)(g.hs + g.ts) + (size_t)g.nz * g.bs + (size_t)nwb * g.nx * g.ast);
+         (8 + 3 * (size_t)(g.hs + g.ts + 4) + (size_t)g.nz * g.bs + (size_t)nwb * g.nx * g.ast);
 }
 
 // launch shapes of k_zfwd / k_zadj: NT tasks of W outputs per thread, NTH
@@ -97,7 +98,7 @@ struct ZShape {
   int nt, nth, w, fwd;
 };
 constexpr int kZNShapes = 13;
-constexpr ZShape kZShapes[kZNShapes] = {{1, 512, 8, 1},  {2, 512, 8, 1},  {3, 512, 8, 1},   {4, 512, 8, 1},
+constexpr ZShape kZShapes[kZNShapes] = {{1, 512, 8, 1},  {2, 512, 8, 1},  {3, 512, 8, 1},   {4, 512, 8, 0},
                                         {1, 640, 8, 1},  {2, 640, 8, 1},  {3, 640, 8, 0},   {1, 1024, 8, 0},
                                         {1, 512, 16, 1}, {2, 512, 16, 1}, {1, 640, 16, 1},  {2, 640, 16, 0},
                                         {1, 1024, 16, 0}};
