@@ -751,7 +751,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 // Epilogue (IZ layout): v = acc (+ prev); mode 1: zeros -> +Inf; mode 2:
 // v = x * (v / asum); out = v (z < nz only; out may be prev or x).
 template <int ZPL>
-__global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restrict__ T,
+__global__ void __launch_bounds__(256, (ZPL <= 14 ? 4 : 2)) k_zrot_adj(ZGeom g, const float* __restrict__ T,
                                                  const float4* __restrict__ rot, const int* __restrict__ vidx, int nv,
                                                  const float* prev, float* out, const float* x,
                                                  const float* __restrict__ asum, int mode) {
@@ -768,7 +768,10 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
     float2 acc[ZPL / 2];
 #pragma unroll
     for (int q = 0; q < ZPL / 2; ++q) acc[q] = make_float2(0.f, 0.f);
-    for (int s = half; s < nv; s += 2) {
+    // every lane runs the same number of rounds (the shuffles need them all)
+    for (int s0 = 0; s0 < nv; s0 += 2) {
+      const bool live = s0 + half < nv;
+      const int s = live ? s0 + half : s0;
       const float4 r = rot[vidx[s]];
       const float cs = r.x, sn = r.y;
       const float d1 = fj1 - c0, d2 = fj2 - c0;
@@ -777,42 +780,43 @@ __global__ void __launch_bounds__(256) k_zrot_adj(ZGeom g, const float* __restri
       const int xlo = max(0, (int)ceilf(xc - rr)), xhi = min(nx - 1, (int)floorf(xc + rr));
       const int ylo = max(0, (int)ceilf(yc - rr)), yhi = min(ny - 1, (int)floorf(yc + rr));
       const float* Ts = T + (size_t)s * ny * nx * nzp + 2 * lane;
-      // the candidates first (weights, column offsets; 0 for the invalid
-      // ones), then their loads, so that a group has all of them in flight
-      float cw[9];
-      int co[9];
+      // candidate c = 3 i + k (x offset i, y offset k): weight and column
+      // offset (-1: no footprint), with the forward's own operations
+      auto cand = [&](int c, float& w, int& o) {
+        const int i = (c * 11) >> 5, k = c - 3 * i;  // c / 3 for c <= 8
+        const int xx = min(xlo + i, nx - 1), yy = min(ylo + k, ny - 1);
+        const float di = __fsub_rn((float)xx, c0), dj = __fsub_rn((float)yy, c0);
+        const float s1 = __fadd_rn(c0, __fsub_rn(__fmul_rn(cs, di), __fmul_rn(sn, dj)));
+        const float s2 = __fadd_rn(c0, __fadd_rn(__fmul_rn(sn, di), __fmul_rn(cs, dj)));
+        const bool ok = live && xlo + i <= xhi && ylo + k <= yhi && s1 >= fj1 - 1.f && s1 < fj1 + 1.f &&
+                        s2 >= fj2 - 1.f && s2 < fj2 + 1.f;
+        const float f1 = floorf(s1), f2 = floorf(s2);
+        const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
+        const float a1 = f1 == fj1 ? __fsub_rn(1.0f, t1) : t1;
+        const float a2 = f2 == fj2 ? __fsub_rn(1.0f, t2) : t2;
+        w = ok ? __fmul_rn(a1, a2) : 0.f;
+        o = ok ? (yy * nx + xx) * nzp : -1;
+      };
+      // lane l of the group evaluates candidate l, every lane candidate 8;
+      // the group shares them by shuffles and sums them in the order c = 0..8
+      float wl, w8;
+      int ol, o8;
+      cand(lane, wl, ol);
+      cand(8, w8, o8);
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        const int xx = min(xlo + i, nx - 1);
-        const float di = __fsub_rn((float)xx, c0);
-        const float ca = __fmul_rn(cs, di), cc = __fmul_rn(sn, di);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          const int yy = min(ylo + k, ny - 1);
-          const float dj = __fsub_rn((float)yy, c0);
-          const float s1 = __fadd_rn(c0, __fsub_rn(ca, __fmul_rn(sn, dj)));
-          const float s2 = __fadd_rn(c0, __fadd_rn(cc, __fmul_rn(cs, dj)));
-          const bool ok = xlo + i <= xhi && ylo + k <= yhi && s1 >= fj1 - 1.f && s1 < fj1 + 1.f &&
-                          s2 >= fj2 - 1.f && s2 < fj2 + 1.f;
-          const float f1 = floorf(s1), f2 = floorf(s2);
-          const float t1 = __fsub_rn(s1, f1), t2 = __fsub_rn(s2, f2);
-          const float a1 = f1 == fj1 ? __fsub_rn(1.0f, t1) : t1;
-          const float a2 = f2 == fj2 ? __fsub_rn(1.0f, t2) : t2;
-          cw[3 * i + k] = ok ? __fmul_rn(a1, a2) : 0.f;
-          co[3 * i + k] = ok ? (yy * nx + xx) * nzp : -1;
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < 9; ++c)
-        if (co[c] >= 0) {
-          const float* tp = Ts + co[c];
+      for (int c = 0; c < 9; ++c) {
+        const float w = c < 8 ? __shfl_sync(0xffffffffu, wl, c, 8) : w8;
+        const int o = c < 8 ? __shfl_sync(0xffffffffu, ol, c, 8) : o8;
+        if (o >= 0) {
+          const float* tp = Ts + o;
 #pragma unroll
           for (int q = 0; q < ZPL / 2; ++q) {
             const float2 t = *reinterpret_cast<const float2*>(tp + 16 * q);
-            acc[q].x = fmaf(cw[c], t.x, acc[q].x);
-            acc[q].y = fmaf(cw[c], t.y, acc[q].y);
+            acc[q].x = fmaf(w, t.x, acc[q].x);
+            acc[q].y = fmaf(w, t.y, acc[q].y);
           }
         }
+      }
     }
 #pragma unroll
     for (int q = 0; q < ZPL / 2; ++q) {  // even + odd slots
