@@ -165,6 +165,9 @@ def peaks(S, L):
             "hbm_gbs": hbm, "hbm_source": src}
 
 
+PATH_NAMES = {"fused": "fused projector pair", "strip": "large-plane pass kernels", "split": "split kernels"}
+
+
 def launch_work(plan, kind, nv):
     """(kernel name, bound, algorithmic FLOPs, algorithmic bytes, executed
     FLOPs or None) of one launch of kernel kind `kind` processing nv views,
@@ -184,7 +187,19 @@ def launch_work(plan, kind, nv):
     Npx = 1 << int(np.ceil(np.log2(nx + px - 1)))
     Npz = 1 << int(np.ceil(np.log2(nz + pz - 1)))
     F = fft_flops(nv, ny, Npx, Npz)
-    if plan.fused:
+    path = plan.path
+    if path == "strip":  # two launches per pass: gather + z pass, x pass (forward); x pass, z pass (adjoint)
+        tz, tx = plan.conv_taps()
+        table = {
+            "k_conv_fwd": ("k_zs_fz|k_zs_fx", "fp32", F / 2, 4.0 * (nv * ny * nx * nzp + N + 2 * nv * N) / 2,
+                           nv * ny * nx * nz * (2.0 * (tx + tz) + 8) / 2),
+            "k_conv_adj": ("k_zs_ax|k_zs_az", "fp32", F / 2, 4.0 * (2 * nv * ny * nx * nzp + nv * nxz + 2 * nv * N) / 2,
+                           nv * ny * nx * nz * (2.0 * (tx + tz) + 1) / 2),
+            "k_rot_adj": ("k_zrot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * ny * nx * nzp + 3 * N), None),
+            "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz, None),
+            "k_reduce_image": ("k_from_iz", "hbm", 0.0, 4.0 * 2 * N, None),
+        }
+    elif path == "fused":
         tz, tx = plan.conv_taps()
         table = {
             "k_conv_fwd": ("k_zfwd", "fp32", F, 4.0 * (nv * ny * nx * nzp + N), nv * ny * nx * nz * (2.0 * (tx + tz) + 8)),
@@ -383,7 +398,7 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded phantoms)",
         "config": dict(CONFIG),
-        "path": ("fused projector pair" if plan.fused else "split kernels") + " (device-resident OS-EM), autotuned",
+        "path": PATH_NAMES[plan.path] + " (device-resident OS-EM), autotuned",
         "convolution": {"forward": conv["forward"], "adjoint": conv["adjoint"],
                         "taps_per_plane_z_x": [round(t, 2) for t in plan.conv_taps()], "psf_taps_z_x": [plan.pz, plan.px]},
         "parity": parity,
@@ -674,7 +689,7 @@ def run_study(S, L, torch, name, args, pk, flush):
             e2e.append(time.perf_counter() - t0)
     res = {"workload": f"{name}: {st.nview} views, {plan.px}x{plan.pz} PSF, "
                        f"{'ML-EM' if nb == 1 else f'OS-EM {nb} subsets'} x {niter} iterations",
-           "path": "fused projector pair" if plan.fused else "split kernels",
+           "path": PATH_NAMES[plan.path],
            "recons_per_s": round(1e3 * steps / float(np.sum(times)), 3), "ms_per_recon": round(float(np.mean(times)), 3),
            "e2e_recons_per_s": round(len(e2e) / float(np.sum(e2e)), 3),
            "h2d_bytes": int(4 * (nx * ny * nz + 2 * nx * nz * st.nview)), "d2h_bytes": int(4 * nx * ny * nz),

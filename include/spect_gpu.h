@@ -98,10 +98,13 @@ int spect_plan_conv_kernels(spect_plan_t plan, int out[4]);
 /* 1 in *fused when the plan runs the fused projector pair (rotation,
  * attenuation, separable PSF convolution and depth sum in one forward kernel;
  * the adjoint convolution then an atomic-free gather rotation adjoint with
- * the EM update fused), 0 when it runs the split kernels.  The fused pair is
- * used for :two plans with the attenuation cache, rank-1 PSF planes and planes
- * that fit in shared memory (SPECT_ZPATH=0 turns it off).  No counterpart in
- * the reference (query of this implementation's kernel choice). */
+ * the EM update fused); 2 when it runs the large-plane kernels (the same
+ * layouts and passes, one kernel per pass over plane tiles: planes too large
+ * for the fused kernels' shared memory; SPECT_ZSTRIP=1 prefers them, =0 never
+ * takes them); 0 when it runs the split kernels.  1 and 2 are used for :two
+ * plans with the attenuation cache and rank-1 PSF planes of at most 69 taps
+ * (SPECT_ZPATH=0 turns both off).  No counterpart in the reference (query of
+ * this implementation's kernel choice). */
 int spect_plan_fused(spect_plan_t plan, int* fused);
 
 /* taps[0], taps[1]: mean number of PSF taps per depth plane that the plan's

@@ -203,7 +203,17 @@ class SPECTplan:
         kernel; gather rotation adjoint with the EM update fused)."""
         out = ctypes.c_int(0)
         check(_native.lib().spect_plan_fused(self._h, ctypes.byref(out)))
-        return bool(out.value)
+        return out.value == 1
+
+    @property
+    def path(self):
+        """Which kernels the plan runs: "fused" (the fused projector pair),
+        "strip" (the same layouts and passes as one kernel per pass over plane
+        tiles, for planes too large for the fused kernels' shared memory) or
+        "split" (rotation, convolution and reduction kernels)."""
+        out = ctypes.c_int(0)
+        check(_native.lib().spect_plan_fused(self._h, ctypes.byref(out)))
+        return ("split", "fused", "strip")[out.value]
 
     def conv_taps(self):
         """Mean PSF taps per depth plane that the z and x convolution passes

@@ -237,6 +237,13 @@ struct spect_plan_s {
   int* d_Rz = nullptr;         // [nset][ny][8] tap-block ranges of the four passes
   double ztaps[2] = {0, 0};    // mean kept taps per plane of the fused passes (z, x)
   int zshape_fwd = -1, zshape_adj = -1;
+  // large-plane kernels (zpath == 2): task width, column / row tiles, shared
+  // memory and resident blocks per SM of k_zs_fz, k_zs_fx, k_zs_ax, k_zs_az,
+  // and the plane-tile exchange buffer
+  int zs_w = 8, zs_tx = 8, zs_tz = 4;
+  size_t zs_smem[4] = {0, 0, 0, 0};
+  int zs_occ[4] = {1, 1, 1, 1};
+  float* d_Q = nullptr;
   // split kernels with the gather rotation adjoint: the premultiplied adjoint
   // planes are transposed into d_Tz (z fastest) and gathered into d_backIZ
   int gadj = 0;
@@ -271,7 +278,7 @@ void free_plan(spect_plan_s* p) {
   void* ptrs[] = {p->d_mumap, p->d_att, p->d_err, p->d_r1view, p->d_R1, p->d_gscr_r1, p->d_H,     p->d_rot,      p->d_viewset,   p->d_tw,         p->d_all,
                   p->d_idx,   p->d_P,     p->d_part,     p->d_Vs,      p->d_imgpart,    p->d_gB,
                   p->d_gacc,  p->d_gscr_adj, p->d_views_tmp, p->d_ones, p->d_asum,       p->d_flag, p->d_sub,
-                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep, p->d_imgIZ, p->d_backIZ, p->d_Hz, p->d_Ez, p->d_Tz, p->d_Rz};
+                  p->d_io_img, p->d_io_views, p->d_Hsep, p->d_Tsep, p->d_imgIZ, p->d_backIZ, p->d_Hz, p->d_Ez, p->d_Tz, p->d_Rz, p->d_Q};
   for (void* q : ptrs)
     if (q) {
       if (p->async_alloc) cudaFreeAsync(q, p->home);
@@ -554,22 +561,47 @@ ZArgs zargs(const spect_plan_s* p) {
 
 // zpath forward of nidx views of the IZ image: k_zfwd (rotation, attenuation,
 // convolution, depth sum of chunks) then the chunk sum (+ EM ratio y/(Ax+bg))
+// depth chunks of the large-plane kernels over nv views and `tiles` row
+// tiles: about two work items per SM, at most nchunk_max chunks
+void zs_chunking(const spect_plan_s* p, int nv, int tiles, int* chunkY, int* nchunks) {
+  int nc = std::max(1, std::min(p->ny, cdiv(2 * p->sm_count, std::max(1, nv * tiles))));
+  nc = std::min(nc, (int)p->nchunk_max);
+  *chunkY = cdiv(p->ny, nc);
+  *nchunks = cdiv(p->ny, *chunkY);
+}
+
 int zforward(spect_plan_s* p, float* views, const float* imgIZ, const int* vidx, int nidx, cudaStream_t st,
              const float* y, const float* bg, float* partbuf, int gmax) {
   for (int g0 = 0; g0 < nidx; g0 += gmax) {
     const int nv = std::min(gmax, nidx - g0);
     const int* vi = vidx + g0;
     int cy, nc;
-    chunking(p, nv, false, &cy, &nc);
     ZArgs a = zargs(p);
     a.img = imgIZ;
     a.vidx = vi;
     a.nv = nv;
-    a.chunkY = cy;
-    a.nchunks = nc;
     a.part = partbuf;
-    const int gs = std::min(p->sm_count, nv * nc);
-    LAUNCH(p, K_CONV_FWD, st, "k_zfwd", zfwd_launch(p->zshape_fwd, gs, p->zfwd_smem_b, st, a));
+    if (p->zpath == 2) {  // large planes: gather + z pass -> Q, x pass + depth sum -> part
+      // the fused kernel's depth chunks: the same partial sums, bit for bit
+      const int ntz = cdiv(p->nz, p->zs_tz);
+      chunking(p, nv, false, &cy, &nc);
+      a.chunkY = cy;
+      a.nchunks = nc;
+      a.Q = p->d_Q;
+      a.tx = p->zs_tx;
+      a.tz = p->zs_tz;
+      const int n1 = nv * p->ny * (p->nx / p->zs_tx), n2 = nv * nc * ntz;
+      LAUNCH(p, K_CONV_FWD, st, "k_zs_fz",
+             zs_fz_launch(p->zs_w, std::min(n1, p->sm_count * p->zs_occ[0]), p->zs_smem[0], st, a));
+      LAUNCH(p, K_CONV_FWD, st, "k_zs_fx",
+             zs_fx_launch(p->zs_w, std::min(n2, p->sm_count * p->zs_occ[1]), p->zs_smem[1], st, a));
+    } else {
+      chunking(p, nv, false, &cy, &nc);
+      a.chunkY = cy;
+      a.nchunks = nc;
+      const int gs = std::min(p->sm_count, nv * nc);
+      LAUNCH(p, K_CONV_FWD, st, "k_zfwd", zfwd_launch(p->zshape_fwd, gs, p->zfwd_smem_b, st, a));
+    }
     const size_t n = (size_t)nv * p->nxz;
     const int rb = (int)std::min<size_t>((n + 255) / 256, (size_t)p->sm_count * 16);
     LAUNCH(p, K_REDUCE_VIEWS, st, "k_reduce_views",
@@ -593,16 +625,31 @@ int zbackward(spect_plan_s* p, float* outIZ, const float* views, const int* vidx
     const int nv = std::min(p->gmax, nidx - g0);
     const int* vi = vidx + g0;
     int cy, nc;
-    chunking(p, nv, true, &cy, &nc);
     ZArgs a = zargs(p);
     a.views = views + (size_t)g0 * p->nxz;
     a.T = p->d_P;
     a.vidx = vi;
     a.nv = nv;
-    a.chunkY = cy;
-    a.nchunks = nc;
-    const int gs = std::min(p->sm_count, nv * nc);
-    LAUNCH(p, K_CONV_ADJ, st, "k_zadj", zadj_launch(p->zshape_adj, gs, p->zadj_smem_b, st, a));
+    if (p->zpath == 2) {  // large planes: x pass -> Q, z pass x attenuation -> T
+      const int ntz = cdiv(p->nz, p->zs_tz);
+      zs_chunking(p, nv, ntz, &cy, &nc);
+      a.chunkY = cy;
+      a.nchunks = nc;
+      a.Q = p->d_Q;
+      a.tx = p->zs_tx;
+      a.tz = p->zs_tz;
+      const int n3 = nv * ntz * nc, n4 = nv * p->ny * (p->nx / p->zs_tx);
+      LAUNCH(p, K_CONV_ADJ, st, "k_zs_ax",
+             zs_ax_launch(p->zs_w, std::min(n3, p->sm_count * p->zs_occ[2]), p->zs_smem[2], st, a));
+      LAUNCH(p, K_CONV_ADJ, st, "k_zs_az",
+             zs_az_launch(p->zs_w, std::min(n4, p->sm_count * p->zs_occ[3]), p->zs_smem[3], st, a));
+    } else {
+      chunking(p, nv, true, &cy, &nc);
+      a.chunkY = cy;
+      a.nchunks = nc;
+      const int gs = std::min(p->sm_count, nv * nc);
+      LAUNCH(p, K_CONV_ADJ, st, "k_zadj", zadj_launch(p->zshape_adj, gs, p->zadj_smem_b, st, a));
+    }
     const bool last = g0 + nv >= nidx;
     LAUNCH(p, K_ROT_ADJ, st, "k_zrot_adj",
            zrot_adj_launch(p->zg, grot, st, p->d_P, p->d_rot, vi, nv, g0 > 0 ? p->d_backIZ : nullptr,
@@ -990,7 +1037,7 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
         p->nsplit_adj = kv.second.nsplit_adj;
         p->sep = kv.second.sep && p->sep_fwd_ok;
         p->sep_adj = kv.second.sep_adj && p->sep_adj_ok;
-        if (p->zpath) {
+        if (p->zpath == 1) {
           p->zshape_fwd = kv.second.zshape_fwd;
           p->zshape_adj = kv.second.zshape_adj;
         }
@@ -1013,6 +1060,18 @@ int autotune(spect_plan_s* p, int nv, double* fwd_ms, double* adj_ms) {
   for (double c0 : {0.0, 0.25, 0.5, 1.0, 2.0, 4.0}) {
     int c = best_chunk(p, nv, c0);
     if (std::find(cys.begin(), cys.end(), c) == cys.end()) cys.push_back(c);
+  }
+  if (p->zpath == 2) {
+    // large-plane kernels: their tiles and chunks are fixed by the geometry;
+    // the timings are recorded for the caller
+    double tf = 0, ta = 0;
+    int rc = time_pass(p, false, nv, 2, &tf);
+    if (rc == SPECT_OK) rc = time_pass(p, true, nv, 2, &ta);
+    p->prof.on = prof;
+    if (rc != SPECT_OK) return rc;
+    *fwd_ms = tf;
+    *adj_ms = ta;
+    return SPECT_OK;
   }
   if (p->zpath) {
     // fused path: depth tile and launch shape per direction
@@ -1386,6 +1445,21 @@ void tap_range(const float* w, int len, int* b4, int* n8) {
 // forward -- the fewest thread slots holding every x task of a plane (ties:
 // more threads); adjoint -- the least padded x and z passes, one task per
 // thread and pass
+// tiles of the large-plane kernels: task width w (16 where it divides nx,
+// SPECT_ZW=8 forces 8), column tile tx (32, 16 or 8 dividing nx), row tile
+// tz (a multiple of 4: one x task of w outputs per thread of k_zs_fx and
+// k_zs_ax, tz * nx / w <= kZsNthX); false when a kernel's shared memory
+// does not fit
+bool zs_tiles(const ZGeom& g, size_t optin, ZsTiles* t) {
+  const char* e = std::getenv("SPECT_ZW");
+  t->w = (g.nx % 16 == 0 && !(e && std::atoi(e) == 8)) ? 16 : 8;
+  t->tx = g.nx % 32 == 0 ? 32 : (g.nx % 16 == 0 ? 16 : 8);
+  t->tz = std::min(kZsNthX * t->w / g.nx / 4 * 4, zround(g.nz, 4));
+  if (t->tz < 4) return false;
+  return zs_fz_smem(g, t->tx) <= optin && zs_fx_smem(g, t->tz) <= optin && zs_ax_smem(g, t->tz) <= optin &&
+         zs_az_smem(g, t->tx) <= optin;
+}
+
 // shapes allowed by the geometry and by SPECT_ZW=8|16 (fixes the task width)
 bool zshape_allowed(const ZGeom& g, int i) {
   const char* e = std::getenv("SPECT_ZW");
@@ -1503,18 +1577,30 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
   const bool only_fft = conv_env && std::strcmp(conv_env, "fft") == 0;
   const int pad_rot = (int)std::ceil(1.0 + nx * std::sqrt(2.0) / 2.0 - nx / 2.0);
   const ZGeom zg = zgeom_make(nx, ny, nz, px, pz, pad_rot);
-  bool zcand = false;
+  // zkind 1: the fused pair; 2: the large-plane kernels on the same layouts
+  // (planes too large for the fused kernels' shared memory; SPECT_ZSTRIP=1
+  // prefers them, =0 never takes them); 0: the split kernels
+  int zkind = 0;
+  ZsTiles zt{};
   {
     int dev = 0, optin = 0;
     const char* zenv = std::getenv("SPECT_ZPATH");
+    const char* senv = std::getenv("SPECT_ZSTRIP");
     if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess)
-      zcand = interpmeth == SPECT_INTERP_TWO && sep_host && !only_fft && !(zenv && zenv[0] == '0') && nx % 8 == 0 &&
-              zg.zpw <= 72 && zg.xpw <= 72 &&  // pass rows of at most 9 blocks of 8 taps
-              zg.nzp <= 256 && zpick_fwd(zg) >= 0 && zpick_adj(zg) >= 0 && zfwd_smem(zg, 1) <= (size_t)optin &&
-              zadj_smem(zg, 1) <= (size_t)optin && opts.atten_cache != 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) == cudaSuccess &&
+        interpmeth == SPECT_INTERP_TWO && sep_host && !only_fft && !(zenv && zenv[0] == '0') && nx % 8 == 0 &&
+        zg.zpw <= 72 && zg.xpw <= 72 &&  // pass rows of at most 9 blocks of 8 taps
+        zg.nzp <= 256 && opts.atten_cache != 0) {
+      const bool fused = zpick_fwd(zg) >= 0 && zpick_adj(zg) >= 0 && zfwd_smem(zg, 1) <= (size_t)optin &&
+                         zadj_smem(zg, 1) <= (size_t)optin;
+      const bool strip = zs_tiles(zg, (size_t)optin, &zt);
+      if (fused && !(senv && senv[0] == '1')) zkind = 1;
+      else if (strip && !(senv && senv[0] == '0')) zkind = 2;
+      else if (fused) zkind = 1;
+    }
     cudaGetLastError();
   }
+  const bool zcand = zkind != 0;
   // attenuation cache: on when it fits a quarter of the free device memory
   // (and 32 GiB); SPECT_ATTEN_CACHE=0 turns it off (and with it the fused
   // path).  The fused path keeps it z-fastest ([view][y][x][nzp]), the
@@ -1537,11 +1623,25 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
       p->d_att = nullptr;
       g_err.clear();
     }
-    p->zpath = (zcand && p->d_att) ? 1 : 0;
+    p->zpath = (zcand && p->d_att) ? zkind : 0;
   }
   int st = configure(p);
   if (st != SPECT_OK) return bail(st);
-  if (p->zpath) {
+  if (p->zpath == 2) {
+    p->zg = zg;
+    p->izN = (size_t)zg.L * zg.L * zg.nzp;
+    p->zs_w = zt.w;
+    p->zs_tx = zt.tx;
+    p->zs_tz = zt.tz;
+    p->zs_smem[0] = zs_fz_smem(zg, zt.tx);
+    p->zs_smem[1] = zs_fx_smem(zg, zt.tz);
+    p->zs_smem[2] = zs_ax_smem(zg, zt.tz);
+    p->zs_smem[3] = zs_az_smem(zg, zt.tx);
+    cudaError_t ze = zstrip_setup((int)p->max_smem);
+    if (ze == cudaSuccess) ze = zstrip_occupancy(zt.w, p->zs_smem, p->zs_occ);
+    if (ze != cudaSuccess) return bail(fail(SPECT_ERR_CUDA, std::string("large-plane kernel setup: ") + cudaGetErrorString(ze)));
+  }
+  if (p->zpath == 1) {
     p->zg = zg;
     p->izN = (size_t)zg.L * zg.L * zg.nzp;
     p->zshape_fwd = zpick_fwd(zg);
@@ -1610,6 +1710,8 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
   }
   if (p->zpath) {  // IZ volumes (zero ring and z padding) and zeroed adjoint planes
     if ((st = dalloc(p, &p->d_imgIZ, p->izN)) || (st = dalloc(p, &p->d_backIZ, p->izN)))
+      return bail(st);
+    if (p->zpath == 2 && (st = dalloc(p, &p->d_Q, (size_t)p->gmax * slot)))  // plane tiles of the large-plane kernels
       return bail(st);
     cudaError_t e = cudaMemsetAsync(p->d_imgIZ, 0, sizeof(float) * p->izN, p->home);
     if (e == cudaSuccess) e = cudaMemsetAsync(p->d_backIZ, 0, sizeof(float) * p->izN, p->home);
@@ -1928,7 +2030,7 @@ int spect_plan_conv_kernels(spect_plan_t p, int out[4]) {
 
 int spect_plan_fused(spect_plan_t p, int* fused) {
   if (!p || !fused) return fail(SPECT_ERR_ARG, "null pointer argument");
-  *fused = p->zpath;
+  *fused = p->zpath;  // 1: fused pair; 2: large-plane kernels on the same layouts; 0: split kernels
   return SPECT_OK;
 }
 
@@ -2412,7 +2514,7 @@ size_t est_job_bytes(const ServerJob& j, bool att) {
              + 8 * N + 2 * (size_t)j.nview * nxz + (size_t)j.nblocks * N  // imgpart, EM buffers
              + 2 * N + 2 * (size_t)j.nview * nxz;     // job buffers
   if (j.interp == SPECT_INTERP_ONE) f += nsub * N;
-  else f += nsub * (size_t)j.nx * j.nx * ((j.nz + 15) / 16 * 16) + 2 * N;  // z-fastest planes, IZ volumes
+  else f += 2 * nsub * (size_t)j.nx * j.nx * ((j.nz + 15) / 16 * 16) + 2 * N;  // z-fastest planes and tiles, IZ volumes
   size_t b = 4 * f + (size_t)j.nview * 32;
   // per-CTA global slabs of large planes (B, spectra accumulators)
   if ((size_t)j.nx * (Q + 1) * 8 + 8192 > 227 * 1024) b += (size_t)148 * j.nx * (Q + 1) * 8;

@@ -42,16 +42,21 @@ def test_config_parity(S, O, nx, nz, nview, p, fwhm, idx):
     assert relerr(b, G32.backproject(y, index=idx)) <= TOL
     assert relerr(b, G64.backproject(y, index=idx)) <= TOL
 
-def test_large_512_planes(S, O):
-    """Largest plane: 256x256x200 image, 65x65 PSF -> 512x512 padded planes.
+@pytest.mark.parametrize("path", ["strip", "split"])
+def test_large_512_planes(S, O, monkeypatch, path):
+    """Largest plane: 256x256x200 image, 65x65 PSF -> 512x512 padded planes,
+    through the large-plane pass kernels (the default here) and through the
+    split kernels (SPECT_ZSTRIP=0: FFT convolution, B in global memory).
 
     At this size the reference's own Float32 adjoint carries ~1.8e-4 of FFT
     round-off (fft_conv_adj! sums all 128+156 padded rows/columns into the edge
     pixels, src/fft_convolve.jl:100-122), so the GPU result is held to 1e-4
     against the Float64 oracle and to the oracle's own f32-vs-f64 error
     against the Float32 oracle."""
+    monkeypatch.setenv("SPECT_ZSTRIP", "1" if path == "strip" else "0")
     st = _study(S, 256, 200, 128, 65, 10.0, (0.0096, 0.015, 0.004), seed=5)
     plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+    assert plan.path == path
     G = O.Geometry(st.mumap, st.psfs, st.dy)
     G64 = O.Geometry(st.mumap, st.psfs, st.dy, dtype=np.float64)
     idx = np.array([17], np.int32)
@@ -164,3 +169,28 @@ def test_wide_psf_takes_split_path(S, O):
     G = O.Geometry(st.mumap, st.psfs, st.dy)
     idx = np.array([0, 5], np.int32)
     assert relerr(S.project(st.image, plan, index=idx), G.project(st.image, index=idx)) <= TOL
+
+
+def test_large_plane_kernels_match_fused_bitwise(S, O, monkeypatch):
+    """The large-plane kernels (one kernel per pass over plane tiles) run every
+    output through the fused kernels' operations in the same order: forced on
+    the single larger study's geometry they give the fused pair's projections,
+    back-projections and OS-EM iterate bit for bit."""
+    st = _study(S, 128, 80, 120, 37, 6.0, (0.0096, 0.015), seed=41)
+    idx = np.array([0, 7, 30, 61, 119], np.int32)
+    rng = np.random.default_rng(9)
+    y = np.asfortranarray(rng.random((128, 80, len(idx))), np.float32)
+    x0 = np.ones(st.image.shape, np.float32, order="F")
+    yn = np.asfortranarray(rng.random((128, 80, 120)) + 0.5, np.float32)
+    bg = np.full(yn.shape, 0.1, np.float32, order="F")
+    out = {}
+    for strip in ("0", "1"):
+        monkeypatch.setenv("SPECT_ZSTRIP", strip)
+        plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
+        assert plan.path == ("strip" if strip == "1" else "fused")
+        out[strip] = (S.project(st.image, plan, index=idx), S.backproject(y, plan, index=idx),
+                      S.osem(x0, yn, bg, S.Ablock(plan, 8), niter=1))
+    for a, b in zip(out["0"], out["1"]):
+        assert np.array_equal(a, b)
+    G = O.Geometry(st.mumap, st.psfs, st.dy)
+    assert relerr(out["1"][0], G.project(st.image, index=idx)) <= TOL
