@@ -188,13 +188,13 @@ def launch_work(plan, kind, nv):
     Npz = 1 << int(np.ceil(np.log2(nz + pz - 1)))
     F = fft_flops(nv, ny, Npx, Npz)
     path = plan.path
-    if path == "strip":  # two launches per pass: gather + z pass, x pass (forward); x pass, z pass (adjoint)
+    if path == "strip":  # forward: two launches per pass (gather + z pass, x pass); adjoint: one
         tz, tx = plan.conv_taps()
         table = {
             "k_conv_fwd": ("k_zs_fz|k_zs_fx", "fp32", F / 2, 4.0 * (nv * ny * nx * nzp + N + 2 * nv * N) / 2,
                            nv * ny * nx * nz * (2.0 * (tx + tz) + 8) / 2),
-            "k_conv_adj": ("k_zs_ax|k_zs_az", "fp32", F / 2, 4.0 * (2 * nv * ny * nx * nzp + nv * nxz + 2 * nv * N) / 2,
-                           nv * ny * nx * nz * (2.0 * (tx + tz) + 1) / 2),
+            "k_conv_adj": ("k_zs_adj", "fp32", F, 4.0 * (2 * nv * ny * nx * nzp + nv * nxz),
+                           nv * ny * nx * nz * (2.0 * (tx + tz) + 1)),
             "k_rot_adj": ("k_zrot_adj", "hbm", 8.0 * nv * N, 4.0 * (nv * ny * nx * nzp + 3 * N), None),
             "k_reduce_views": ("k_reduce_views", "hbm", 2.0 * nv * nxz, 4.0 * 4 * nv * nxz, None),
             "k_reduce_image": ("k_from_iz", "hbm", 0.0, 4.0 * 2 * N, None),

@@ -238,11 +238,11 @@ struct spect_plan_s {
   double ztaps[2] = {0, 0};    // mean kept taps per plane of the fused passes (z, x)
   int zshape_fwd = -1, zshape_adj = -1;
   // large-plane kernels (zpath == 2): task width, column / row tiles, shared
-  // memory and resident blocks per SM of k_zs_fz, k_zs_fx, k_zs_ax, k_zs_az,
-  // and the plane-tile exchange buffer
+  // memory and resident blocks per SM of k_zs_fz, k_zs_fx, k_zs_adj, and the
+  // forward's plane-tile exchange buffer
   int zs_w = 8, zs_tx = 8, zs_tz = 4;
-  size_t zs_smem[4] = {0, 0, 0, 0};
-  int zs_occ[4] = {1, 1, 1, 1};
+  size_t zs_smem[3] = {0, 0, 0};
+  int zs_occ[3] = {1, 1, 1};
   float* d_Q = nullptr;
   // split kernels with the gather rotation adjoint: the premultiplied adjoint
   // planes are transposed into d_Tz (z fastest) and gathered into d_backIZ
@@ -561,10 +561,11 @@ ZArgs zargs(const spect_plan_s* p) {
 
 // zpath forward of nidx views of the IZ image: k_zfwd (rotation, attenuation,
 // convolution, depth sum of chunks) then the chunk sum (+ EM ratio y/(Ax+bg))
-// depth chunks of the large-plane kernels over nv views and `tiles` row
-// tiles: about two work items per SM, at most nchunk_max chunks
+// depth chunks of the large-plane adjoint over nv views and `tiles` column
+// tiles: about four work items per SM (a short last wave), at most
+// nchunk_max chunks
 void zs_chunking(const spect_plan_s* p, int nv, int tiles, int* chunkY, int* nchunks) {
-  int nc = std::max(1, std::min(p->ny, cdiv(2 * p->sm_count, std::max(1, nv * tiles))));
+  int nc = std::max(1, std::min(p->ny, cdiv(4 * p->sm_count, std::max(1, nv * tiles))));
   nc = std::min(nc, (int)p->nchunk_max);
   *chunkY = cdiv(p->ny, nc);
   *nchunks = cdiv(p->ny, *chunkY);
@@ -630,19 +631,14 @@ int zbackward(spect_plan_s* p, float* outIZ, const float* views, const int* vidx
     a.T = p->d_P;
     a.vidx = vi;
     a.nv = nv;
-    if (p->zpath == 2) {  // large planes: x pass -> Q, z pass x attenuation -> T
-      const int ntz = cdiv(p->nz, p->zs_tz);
-      zs_chunking(p, nv, ntz, &cy, &nc);
+    if (p->zpath == 2) {  // large planes: column tiles, x pass and z pass x attenuation -> T
+      const int ntx = p->nx / p->zs_tx;
+      zs_chunking(p, nv, ntx, &cy, &nc);
       a.chunkY = cy;
       a.nchunks = nc;
-      a.Q = p->d_Q;
       a.tx = p->zs_tx;
-      a.tz = p->zs_tz;
-      const int n3 = nv * ntz * nc, n4 = nv * p->ny * (p->nx / p->zs_tx);
-      LAUNCH(p, K_CONV_ADJ, st, "k_zs_ax",
-             zs_ax_launch(p->zs_w, std::min(n3, p->sm_count * p->zs_occ[2]), p->zs_smem[2], st, a));
-      LAUNCH(p, K_CONV_ADJ, st, "k_zs_az",
-             zs_az_launch(p->zs_w, std::min(n4, p->sm_count * p->zs_occ[3]), p->zs_smem[3], st, a));
+      LAUNCH(p, K_CONV_ADJ, st, "k_zs_adj",
+             zs_adj_launch(p->zs_w, std::min(nv * ntx * nc, p->sm_count * p->zs_occ[2]), p->zs_smem[2], st, a));
     } else {
       chunking(p, nv, true, &cy, &nc);
       a.chunkY = cy;
@@ -1447,17 +1443,15 @@ void tap_range(const float* w, int len, int* b4, int* n8) {
 // thread and pass
 // tiles of the large-plane kernels: task width w (16 where it divides nx,
 // SPECT_ZW=8 forces 8), column tile tx (32, 16 or 8 dividing nx), row tile
-// tz (a multiple of 4: one x task of w outputs per thread of k_zs_fx and
-// k_zs_ax, tz * nx / w <= kZsNthX); false when a kernel's shared memory
-// does not fit
+// tz (a multiple of 4: one x task of w outputs per thread of k_zs_fx,
+// tz * nx / w <= kZsNthX); false when a kernel's shared memory does not fit
 bool zs_tiles(const ZGeom& g, size_t optin, ZsTiles* t) {
   const char* e = std::getenv("SPECT_ZW");
   t->w = (g.nx % 16 == 0 && !(e && std::atoi(e) == 8)) ? 16 : 8;
   t->tx = g.nx % 32 == 0 ? 32 : (g.nx % 16 == 0 ? 16 : 8);
   t->tz = std::min(kZsNthX * t->w / g.nx / 4 * 4, zround(g.nz, 4));
   if (t->tz < 4) return false;
-  return zs_fz_smem(g, t->tx) <= optin && zs_fx_smem(g, t->tz) <= optin && zs_ax_smem(g, t->tz) <= optin &&
-         zs_az_smem(g, t->tx) <= optin;
+  return zs_fz_smem(g, t->tx) <= optin && zs_fx_smem(g, t->tz) <= optin && zs_adj_smem(g, t->tx) <= optin;
 }
 
 // shapes allowed by the geometry and by SPECT_ZW=8|16 (fixes the task width)
@@ -1635,8 +1629,7 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     p->zs_tz = zt.tz;
     p->zs_smem[0] = zs_fz_smem(zg, zt.tx);
     p->zs_smem[1] = zs_fx_smem(zg, zt.tz);
-    p->zs_smem[2] = zs_ax_smem(zg, zt.tz);
-    p->zs_smem[3] = zs_az_smem(zg, zt.tx);
+    p->zs_smem[2] = zs_adj_smem(zg, zt.tx);
     cudaError_t ze = zstrip_setup((int)p->max_smem);
     if (ze == cudaSuccess) ze = zstrip_occupancy(zt.w, p->zs_smem, p->zs_occ);
     if (ze != cudaSuccess) return bail(fail(SPECT_ERR_CUDA, std::string("large-plane kernel setup: ") + cudaGetErrorString(ze)));

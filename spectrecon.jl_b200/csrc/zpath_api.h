@@ -114,17 +114,14 @@ __host__ __device__ inline size_t zs_fz_smem(const ZGeom& g, int tx) {
 __host__ __device__ inline size_t zs_fx_smem(const ZGeom& g, int tz) {
   return sizeof(float) * 2 * ((size_t)tz * g.bs + g.hs + g.ts + 4);
 }
-__host__ __device__ inline size_t zs_ax_smem(const ZGeom& g, int tz) {
-  return sizeof(float) * ((size_t)tz * g.bs + (size_t)g.nx * (tz + 4) + g.hs + g.ts + 4);
-}
-__host__ __device__ inline size_t zs_az_smem(const ZGeom& g, int tx) {
-  return sizeof(float) * ((size_t)tx * g.ast + g.hs + g.ts + 4);
+__host__ __device__ inline size_t zs_adj_smem(const ZGeom& g, int tx) {
+  return sizeof(float) * ((size_t)g.nz * zstride4(tx + g.xpw) + (size_t)tx * g.ast + g.hs + g.ts + 4);
 }
 struct ZsTiles {
   int w, tx, tz;  // task width, column tile, row tile
 };
-constexpr int kZsNth = 512;   // k_zs_fz, k_zs_az threads
-constexpr int kZsNthX = 640;  // k_zs_fx, k_zs_ax threads (one x task each)
+constexpr int kZsNth = 512;   // k_zs_fz, k_zs_adj threads
+constexpr int kZsNthX = 640;  // k_zs_fx threads (one x task each)
 
 // launchers (zpath_inst.cu)
 cudaError_t zpath_setup(int max_smem);
@@ -138,13 +135,13 @@ cudaError_t zt_to_z_launch(const ZGeom& g, int planes, cudaStream_t st, const fl
                             const float* att, const int* vidx);
 cudaError_t zfrom_iz_launch(const ZGeom& g, cudaStream_t st, const float* iz, float* dst, const float* asum, int mode);
 // large-plane kernels: w = task width (8 or 16); occ = resident blocks per
-// SM of each kernel at its shared-memory size (for the persistent grids)
+// SM of k_zs_fz, k_zs_fx, k_zs_adj at their shared-memory sizes (for the
+// persistent grids)
 cudaError_t zstrip_setup(int max_smem);
-cudaError_t zstrip_occupancy(int w, const size_t smem[4], int occ[4]);
+cudaError_t zstrip_occupancy(int w, const size_t smem[3], int occ[3]);
 cudaError_t zs_fz_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
 cudaError_t zs_fx_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
-cudaError_t zs_ax_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
-cudaError_t zs_az_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
+cudaError_t zs_adj_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
 cudaError_t zatten_launch(const ZGeom& g, int nview, cudaStream_t st, const float* muz, const float4* rot, float dy,
                           float* att);
 

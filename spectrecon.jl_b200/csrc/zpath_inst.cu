@@ -63,8 +63,7 @@ cudaError_t zrot_adj_launch(const ZGeom& g, int grid, cudaStream_t st, const flo
 namespace {
 const void* const kZsFz[2] = {(const void*)k_zs_fz<kZsNth, 8>, (const void*)k_zs_fz<kZsNth, 16>};
 const void* const kZsFx[2] = {(const void*)k_zs_fx<kZsNthX, 8>, (const void*)k_zs_fx<kZsNthX, 16>};
-const void* const kZsAx[2] = {(const void*)k_zs_ax<kZsNthX, 8>, (const void*)k_zs_ax<kZsNthX, 16>};
-const void* const kZsAz[2] = {(const void*)k_zs_az<kZsNth, 8>, (const void*)k_zs_az<kZsNth, 16>};
+const void* const kZsAdj[2] = {(const void*)k_zs_adj<kZsNth, 8>, (const void*)k_zs_adj<kZsNth, 16>};
 cudaError_t zs_launch(const void* k, int nth, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
   ZArgs c = a;
   void* args[] = {&c};
@@ -74,18 +73,18 @@ cudaError_t zs_launch(const void* k, int nth, int grid, size_t smem, cudaStream_
 
 cudaError_t zstrip_setup(int max_smem) {
   for (int i = 0; i < 2; ++i)
-    for (const void* k : {kZsFz[i], kZsFx[i], kZsAx[i], kZsAz[i]}) {
+    for (const void* k : {kZsFz[i], kZsFx[i], kZsAdj[i]}) {
       const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
       if (e != cudaSuccess) return e;
     }
   return cudaSuccess;
 }
 
-cudaError_t zstrip_occupancy(int w, const size_t smem[4], int occ[4]) {
+cudaError_t zstrip_occupancy(int w, const size_t smem[3], int occ[3]) {
   const int i = w == 16 ? 1 : 0;
-  const void* ks[4] = {kZsFz[i], kZsFx[i], kZsAx[i], kZsAz[i]};
-  const int nth[4] = {kZsNth, kZsNthX, kZsNthX, kZsNth};
-  for (int j = 0; j < 4; ++j) {
+  const void* ks[3] = {kZsFz[i], kZsFx[i], kZsAdj[i]};
+  const int nth[3] = {kZsNth, kZsNthX, kZsNth};
+  for (int j = 0; j < 3; ++j) {
     const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[j], ks[j], nth[j], smem[j]);
     if (e != cudaSuccess) return e;
     if (occ[j] < 1) occ[j] = 1;
@@ -99,11 +98,8 @@ cudaError_t zs_fz_launch(int w, int grid, size_t smem, cudaStream_t st, const ZA
 cudaError_t zs_fx_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
   return zs_launch(kZsFx[w == 16 ? 1 : 0], kZsNthX, grid, smem, st, a);
 }
-cudaError_t zs_ax_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
-  return zs_launch(kZsAx[w == 16 ? 1 : 0], kZsNthX, grid, smem, st, a);
-}
-cudaError_t zs_az_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
-  return zs_launch(kZsAz[w == 16 ? 1 : 0], kZsNth, grid, smem, st, a);
+cudaError_t zs_adj_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
+  return zs_launch(kZsAdj[w == 16 ? 1 : 0], kZsNth, grid, smem, st, a);
 }
 
 cudaError_t zto_iz_launch(const ZGeom& g, cudaStream_t st, const float* img, float* iz) {

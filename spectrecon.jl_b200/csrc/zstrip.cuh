@@ -2,8 +2,8 @@
 // kernels' shared memory (e.g. 256x256x200 with a 65-tap PSF), on the same
 // z-fastest layouts (IZ image, ATT cache, T adjoint planes) and with the same
 // trimmed separable passes (zpassw, tail and fold tables, tap ranges) as
-// zpath.cuh; each pass is a kernel of its own over plane tiles, and the
-// passes exchange planes through the device buffer Q.
+// zpath.cuh, over plane tiles; the forward's two passes are kernels of their
+// own that exchange planes through the device buffer Q.
 //
 // forward (project!, src/project.jl:77-135):
 //   k_zs_fz  item (slot, y, tile of tx columns): gather the rotated,
@@ -12,9 +12,8 @@
 //            Q (loaded one plane ahead into registers), x pass accumulated
 //            over the chunk -> part[slot][chunk][z][x]
 // adjoint (backproject!, src/backproject.jl:69-124), convolution half:
-//   k_zs_ax  item (slot, tile of tz rows, depth chunk): the view's rows once;
-//            per plane the x pass -> Q[slot][y][x][nzp] (columns, z fastest)
-//   k_zs_az  item (slot, y, tile of tx columns): the columns of Q, z pass,
+//   k_zs_adj item (slot, tile of tx columns, depth chunk): the view's columns
+//            of the tile and its halo once; per plane the x pass, the z pass
 //            times the attenuation -> T[slot][y][x][nzp]
 // Every output goes through the operations of the fused kernels in the same
 // order (z then x in the forward, x then z in the adjoint), so the two paths
@@ -253,135 +252,96 @@ __global__ void __launch_bounds__(NTH, 1) k_zs_fx(ZArgs a) {
 }
 
 // ------------------------------------------------------------------------
-// k_zs_ax<NTH, W>: adjoint x pass, one task of W outputs per thread and
-// plane (tz * nx / W <= NTH).  Shared memory (floats): [VB tz * bs (data
-// columns C0..)][OB nx * (tz + 4): column x, row zl][table hs + ts + 4].
+// k_zs_adj<NTH, W>: adjoint convolution of a tile of tx columns; item =
+// (slot, column tile, depth chunk).  The view's columns X0 - C0 .. X0 + tx +
+// xpw - C0 (zero outside the image) are loaded once per item as the tile's
+// zero-padded lines, the same values at the same shifted positions as
+// k_zadj's full rows; per plane the x pass (tx / W tasks a row) -> WB, the z
+// pass times the attenuation -> T.  Shared memory (floats): [VB nz * tbs]
+// [WB tx * ast: column x, data rows R0..][table hs + ts + 4], tbs =
+// zstride4(tx + xpw).
 template <int NTH, int W>
-__global__ void __launch_bounds__(NTH) k_zs_ax(ZArgs a) {
+__global__ void __launch_bounds__(NTH) k_zs_adj(ZArgs a) {
   extern __shared__ float4 smem4[];
   const ZGeom& g = a.g;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts, tz = a.tz, bs = g.bs;
-  const int C0 = g.C0, hx = g.hx, obs = tz + 4;
+  const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts, tx = a.tx;
+  const int ast = g.ast, R0 = g.R0, C0 = g.C0, hz = g.hz, hx = g.hx, tbs = zstride4(tx + g.xpw);
   float* const VB = reinterpret_cast<float*>(smem4);
-  float* const OB = VB + tz * bs;
-  float* const Wt = OB + nx * obs;
+  float* const WB = VB + (size_t)nz * tbs;
+  float* const Wt = WB + (size_t)tx * ast;
   const int tid = threadIdx.x;
-  const int ntz = (nz + tz - 1) / tz, nitems = a.nv * ntz * a.nchunks, xbs = nx / W, t4 = tz / 4;
-  const float rtz = 1.0f / tz, rbs = 1.0f / bs, rt4 = 1.0f / t4;
-  const int xb = zdiv(tid, rtz), zl = tid - xb * tz, x0 = W * xb;
+  const int ntx = nx / tx, nitems = a.nv * ntx * a.nchunks, nzb = (nz + W - 1) / W;
+  const int xbs = tx / W, xtasks = nz * xbs, ztasks = tx * nzb;
+  const float rnz = 1.0f / nz, rtx = 1.0f / tx, rtbs = 1.0f / tbs;
+  for (int k = tid; k < tx * ast; k += NTH) WB[k] = 0.f;  // rows outside the data stay zero
   for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int ch = item % a.nchunks, st = item / a.nchunks, slot = st / ntz, zt = st - slot * ntz;
-    const int Z0 = zt * tz, rows = min(tz, nz - Z0);
-    const int y0 = ch * a.chunkY, y1 = min(ny, y0 + a.chunkY);
+    const int ch = item % a.nchunks, st = item / a.nchunks, slot = st / ntx, xt = st - slot * ntx;
+    const int X0 = xt * tx, y0 = ch * a.chunkY, y1 = min(ny, y0 + a.chunkY);
     const int v = a.vidx[slot], set = a.viewset[v];
-    const bool mine = tid < tz * xbs && zl < rows;
-    // the view's rows Z0 .. Z0 + rows - 1, zero-padded (the previous item's
-    // last pass ended at a barrier)
-    const float* V = a.views + ((size_t)slot * nz + Z0) * nx;
-    for (int e = tid; e < tz * bs; e += NTH) {
-      const int z = zdiv(e, rbs), c = e - z * bs;
-      VB[e] = (z < rows && c >= C0 && c < C0 + nx) ? V[(size_t)z * nx + c - C0] : 0.f;
+    // the tile's lines: VB[z][c] = view[z][X0 + c - C0] inside the image, else
+    // zero (the previous item's last pass ended at a barrier)
+    const float* V = a.views + (size_t)slot * nz * nx;
+    for (int e = tid; e < nz * tbs; e += NTH) {
+      const int z = zdiv(e, rtbs), c = e - z * tbs, xg = X0 + c - C0;
+      VB[e] = (xg >= 0 && xg < nx) ? V[(size_t)z * nx + xg] : 0.f;
     }
     for (int y = y0; y < y1; ++y) {
       zs_table(a, set, y, 1, Wt, tid, NTH);
       __syncthreads();
-      if (mine) {
+      // x pass: task (z, x block) -> WB column x, row R0 + z
+      {
         const int2 rg = *reinterpret_cast<const int2*>(Wt + hs + ts + 2);
         const float* cLx = Wt + hs;
         const float* cRx = cLx + hx;
-        const float* row = VB + zl * bs;
-        float o[W];
+        for (int t = tid; t < xtasks; t += NTH) {
+          const int xb = zdiv(t, rnz), z = t - xb * nz, x0 = W * xb;
+          const float* row = VB + z * tbs;
+          float o[W];
 #pragma unroll
-        for (int k = 0; k < W; ++k) o[k] = 0.f;
-        zpassw<W>(Wt + g.zpw, rg.x, rg.y, row + x0, o);
-        if (x0 == 0) o[0] += zfold(cLx, row + C0, 1, hx);
-        if (x0 + W == nx) o[W - 1] += zfold(cRx, row + C0 + nx - 1, -1, hx);
+          for (int k = 0; k < W; ++k) o[k] = 0.f;
+          zpassw<W>(Wt + g.zpw, rg.x, rg.y, row + x0, o);
+          if (X0 + x0 == 0) o[0] += zfold(cLx, row + C0, 1, hx);
+          if (X0 + x0 + W == nx) o[W - 1] += zfold(cRx, row + C0 + x0 + W - 1, -1, hx);
+          float* w = WB + x0 * ast + R0 + z;
 #pragma unroll
-        for (int k = 0; k < W; ++k) OB[(x0 + k) * obs + zl] = o[k];
+          for (int k = 0; k < W; ++k) w[k * ast] = o[k];
+        }
       }
       __syncthreads();
-      // columns -> Q[slot][y][x][Z0 .. Z0 + rows)
-      float* Qp = a.Q + ((size_t)slot * ny + y) * nx * nzp + Z0;
-      if (rows == tz) {
-        for (int e = tid; e < nx * t4; e += NTH) {
-          const int x = zdiv(e, rt4), c = e - x * t4;
-          st4(Qp + (size_t)x * nzp + 4 * c, ld4(OB + x * obs + 4 * c));
+      // z pass: task (x, z block) -> T column (X0 + x, y) of the slot
+      {
+        const int2 rg = *reinterpret_cast<const int2*>(Wt + hs + ts);
+        const float* cLz = Wt + hs + 2 * hx;
+        const float* cRz = cLz + hz;
+        const float* attv = a.att + (((size_t)v * ny + y) * nx + X0) * nzp;
+        float* Tp = a.T + (((size_t)slot * ny + y) * nx + X0) * nzp;
+        for (int t = tid; t < ztasks; t += NTH) {
+          const int zb = zdiv(t, rtx), x = t - zb * tx, z0 = W * zb;
+          float4 at[W / 4];
+#pragma unroll
+          for (int k = 0; k < W / 4; ++k) at[k] = ld4(attv + (size_t)x * nzp + z0 + 4 * k);
+          const float* col = WB + x * ast;
+          float o[W];
+#pragma unroll
+          for (int k = 0; k < W; ++k) o[k] = 0.f;
+          zpassw<W>(Wt, rg.x, rg.y, col + z0, o);
+          if (z0 == 0) o[0] += zfold(cLz, col + R0, 1, hz);
+          if (z0 <= nz - 1 && nz - 1 < z0 + W) {
+            const int kz = nz - 1 - z0;
+            const float s = zfold(cRz, col + R0 + nz - 1, -1, hz);
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+              if (k == kz) o[k] += s;
+          }
+          float* dst = Tp + (size_t)x * nzp + z0;
+#pragma unroll
+          for (int k = 0; k < W / 4; ++k)
+            st4(dst + 4 * k, make_float4(__fmul_rn(at[k].x, o[4 * k]), __fmul_rn(at[k].y, o[4 * k + 1]),
+                                         __fmul_rn(at[k].z, o[4 * k + 2]), __fmul_rn(at[k].w, o[4 * k + 3])));
         }
-      } else {
-        for (int e = tid; e < nx * tz; e += NTH) {
-          const int x = zdiv(e, rtz), c = e - x * tz;
-          if (c < rows) Qp[(size_t)x * nzp + c] = OB[x * obs + c];
-        }
       }
-      // the next round writes the table (read before the last barrier), then
-      // waits at a barrier before its x pass writes OB
+      __syncthreads();
     }
-  }
-}
-
-// ------------------------------------------------------------------------
-// k_zs_az<NTH, W>: adjoint z pass times the attenuation.  Shared memory
-// (floats): [WB tx * ast: column x, data rows R0..][table hs + ts + 4].
-template <int NTH, int W>
-__global__ void __launch_bounds__(NTH) k_zs_az(ZArgs a) {
-  extern __shared__ float4 smem4[];
-  const ZGeom& g = a.g;
-  const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts, tx = a.tx;
-  const int ast = g.ast, R0 = g.R0, hz = g.hz, hx = g.hx;
-  float* const WB = reinterpret_cast<float*>(smem4);
-  float* const Wt = WB + (size_t)tx * ast;
-  const int tid = threadIdx.x;
-  const int ntx = nx / tx, nitems = a.nv * ny * ntx, nz4 = (nz + 3) / 4, nzb = (nz + W - 1) / W;
-  const int ztasks = tx * nzb;
-  const float rnz4 = 1.0f / nz4, rtx = 1.0f / tx;
-  for (int k = tid; k < tx * ast; k += NTH) WB[k] = 0.f;  // rows outside the data stay zero
-  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
-    const int xt = item % ntx, sy = item / ntx, slot = sy / ny, y = sy - slot * ny, X0 = xt * tx;
-    const int v = a.vidx[slot], set = a.viewset[v];
-    zs_table(a, set, y, 1, Wt, tid, NTH);
-    // the tile's columns of Q (rows z < nz only: the rest of WB stays zero)
-    const float* Qp = a.Q + (((size_t)slot * ny + y) * nx + X0) * nzp;
-    for (int e = tid; e < tx * nz4; e += NTH) {
-      const int x = zdiv(e, rnz4), q = e - x * nz4;
-      float4 t = ld4(Qp + (size_t)x * nzp + 4 * q);
-      if (4 * q + 3 >= nz) {
-        if (4 * q + 1 >= nz) t.y = 0.f;
-        if (4 * q + 2 >= nz) t.z = 0.f;
-        t.w = 0.f;
-      }
-      st4(WB + x * ast + R0 + 4 * q, t);
-    }
-    __syncthreads();
-    const int2 rg = *reinterpret_cast<const int2*>(Wt + hs + ts);
-    const float* cLz = Wt + hs + 2 * hx;
-    const float* cRz = cLz + hz;
-    const float* attv = a.att + (((size_t)v * ny + y) * nx + X0) * nzp;
-    float* Tp = a.T + (((size_t)slot * ny + y) * nx + X0) * nzp;
-    for (int t = tid; t < ztasks; t += NTH) {
-      const int zb = zdiv(t, rtx), x = t - zb * tx, z0 = W * zb;
-      float4 at[W / 4];
-#pragma unroll
-      for (int k = 0; k < W / 4; ++k) at[k] = ld4(attv + (size_t)x * nzp + z0 + 4 * k);
-      const float* col = WB + x * ast;
-      float o[W];
-#pragma unroll
-      for (int k = 0; k < W; ++k) o[k] = 0.f;
-      zpassw<W>(Wt, rg.x, rg.y, col + z0, o);
-      if (z0 == 0) o[0] += zfold(cLz, col + R0, 1, hz);
-      if (z0 <= nz - 1 && nz - 1 < z0 + W) {
-        const int kz = nz - 1 - z0;
-        const float s = zfold(cRz, col + R0 + nz - 1, -1, hz);
-#pragma unroll
-        for (int k = 0; k < W; ++k)
-          if (k == kz) o[k] += s;
-      }
-      float* dst = Tp + (size_t)x * nzp + z0;
-#pragma unroll
-      for (int k = 0; k < W / 4; ++k)
-        st4(dst + 4 * k, make_float4(__fmul_rn(at[k].x, o[4 * k]), __fmul_rn(at[k].y, o[4 * k + 1]),
-                                     __fmul_rn(at[k].z, o[4 * k + 2]), __fmul_rn(at[k].w, o[4 * k + 3])));
-    }
-    __syncthreads();
   }
 }
 

@@ -77,14 +77,15 @@ def test_static_scratch_rejects_oversized_plan(S):
     plan.close()
 
 
-@pytest.mark.parametrize("case,env", [("one", {}), ("gauss-fused", {}), ("gauss-split-direct", {"SPECT_ZPATH": "0"}),
+@pytest.mark.parametrize("case,env", [("one", {}), ("gauss-fused", {}), ("gauss-strip", {"SPECT_ZSTRIP": "1"}),
+                                      ("gauss-split-direct", {"SPECT_ZPATH": "0"}),
                                       ("gauss-fft", {"SPECT_CONV": "fft"})])
 def test_static_scratch_kernel_paths(S, O, monkeypatch, case, env):
     """Every kernel path through the static array -- the :one shear rotation,
-    the fused projector pair (Gaussian, hence separable, PSFs), the split
-    direct-convolution kernels and the FFT kernels -- gives spect_project's
-    result on two calls in a row, and the oracle's within the parity
-    tolerance."""
+    the fused projector pair (Gaussian, hence separable, PSFs), the
+    large-plane pass kernels, the split direct-convolution kernels and the
+    FFT kernels -- gives spect_project's result on two calls in a row, and
+    the oracle's within the parity tolerance."""
     import torch
 
     for k, v in env.items():
@@ -99,7 +100,7 @@ def test_static_scratch_kernel_paths(S, O, monkeypatch, case, env):
         psfs = np.asfortranarray(np.repeat(S.psf_gauss(ny=nx, px=11, fwhm_start=1, fwhm_end=3)[:, :, :, None],
                                            nview, axis=3))
         plan = S.SPECTplan(mumap, psfs, 4.8)
-    assert plan.fused == (case == "gauss-fused")
+    assert plan.path == {"gauss-fused": "fused", "gauss-strip": "strip"}.get(case, "split")
     L = S._native.lib()
     x = rng.random((nx, nx, nz)).astype(np.float32)
     image = _dev(torch, x)
