@@ -57,6 +57,10 @@
 #include "bulk_copy.cuh"
 #include "zpath_api.h"
 
+#ifndef ZFWD_GU
+#define ZFWD_GU 2
+#endif
+
 namespace spect {
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
@@ -267,6 +271,7 @@ __global__ void __launch_bounds__(256) k_zatten(ZGeom g, const float* __restrict
 // (rotated, attenuated image -> ZB).
 template <int NT, int NTH, int W>
 __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
+  constexpr int GU = ZFWD_GU;  // gather units per thread and round (4 measured ~1 % faster, with spills in some shapes)
   extern __shared__ float4 smem4[];
   const ZGeom& g = a.g;
   const int nx = g.nx, ny = g.ny, nz = g.nz, nzp = g.nzp, hs = g.hs, ts = g.ts, nsf = g.nsf;
@@ -385,12 +390,12 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
     float* const Hw = Hw0 + hb * hts;
     for (int k = tid; k < hs + ts; k += NTH) Hw[k] = sW[k];
     if (tid < 4) reinterpret_cast<int*>(Hw + hs + ts)[tid] = reinterpret_cast<const int*>(sW + hs + ts)[tid];
-    // two units per round, both units' image loads issued before either is used
-    for (int u0 = tid; u0 < units; u0 += 2 * NTH) {
-      float4 t[2][4];
-      int xs[2], zs[2];
+    // GU units per round, all their image loads issued before any is used
+    for (int u0 = tid; u0 < units; u0 += GU * NTH) {
+      float4 t[GU][4];
+      int xs[GU], zs[GU];
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
+      for (int j = 0; j < GU; ++j) {
         const int u = min(u0 + j * NTH, units - 1);  // a repeated last unit stores the same values
         xs[j] = zdiv(u, rnz4);
         zs[j] = u - xs[j] * nz4;
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zfwd(ZArgs a) {
         t[j][3] = ld4(p + Lz + nzp);
       }
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
+      for (int j = 0; j < GU; ++j) {
         const float4 w = geoW[xs[j]];
         const float4 at = ld4(sA + xs[j] * nzp + 4 * zs[j]);
         const float4 t0 = t[j][0], t1 = t[j][1], t2 = t[j][2], t3 = t[j][3];
