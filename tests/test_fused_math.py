@@ -286,3 +286,41 @@ def test_trimmed_taps_and_ranges(nx, nz, p, f0, f1):
         assert 4 * b4 <= nzi[0] and nzi[-1] < 4 * b4 + 8 * n8
         full, cut = clamp_conv(line, a[::-1]), clamp_conv(line, t[::-1])
         assert np.abs(full - cut).max() <= 2.0 ** -24 * np.abs(full).max()
+
+
+def zs_tiles(g, optin=232448):
+    """Mirror of zs_tiles (csrc/spect_gpu.cu): task width, column tile, row tile."""
+    nx, nz = g["nx"], g["nz"]
+    w = 16 if nx % 16 == 0 else 8
+    tx = 32 if nx % 32 == 0 else (16 if nx % 16 == 0 else 8)
+    tz = min(640 * w // nx // 4 * 4, zround(nz, 4))
+    hts = g["hs"] + g["ts"] + 4
+    smem = {"fz": 4 * (hts + 5 * tx + tx * g["ast"] + nz * tx),
+            "fx": 4 * 2 * (tz * g["bs"] + hts),
+            "adj": 4 * (nz * zstride4(tx + g["xpw"]) + tx * g["ast"] + hts)}
+    return w, tx, tz, smem
+
+
+@pytest.mark.parametrize("nx,nz,px,pz", [(256, 200, 65, 65), (128, 80, 37, 37), (128, 128, 37, 37), (512, 96, 21, 21),
+                                         (64, 37, 9, 9), (96, 48, 21, 21)])
+def test_large_plane_tile_bounds(nx, nz, px, pz):
+    """Every index the large-plane kernels form stays inside its buffer, and
+    their shared memory fits at the benchmark's large study."""
+    g = zgeom(nx, nz, px, pz)
+    w, tx, tz, smem = zs_tiles(g)
+    assert tz >= 4 and tz % 4 == 0 and nx % tx == 0 and tx % 4 == 0 and nx % w == 0
+    # k_zs_fx: one x task per thread, the prefetch holds a plane's rows in four float4 a thread
+    assert tz * (nx // w) <= 640 and tz * nx // 4 <= 4 * 640
+    # its rows: data at C0 .. C0 + nx - 1, windows read x0 .. x0 + xpw + w - 1
+    assert g["C0"] + nx <= g["bs"] and (nx - w) + g["xpw"] + w <= g["bs"]
+    # k_zs_fz / k_zs_adj z pass: column rows as the fused kernels (R0 + 4 nz4 <= ast, windows <= rows)
+    nzb = (nz + w - 1) // w
+    assert g["R0"] + 4 * ((nz + 3) // 4) <= g["ast"] and w * (nzb - 1) + g["zpw"] + w <= g["rows"] <= g["ast"]
+    # k_zs_adj tile lines: windows read x0 .. x0 + xpw + w - 1 (x0 <= tx - w); the left fold
+    # (first tile, x0 = 0) reads C0 .. C0 + hx - 1, the right fold (last tile, x0 = tx - w)
+    # C0 + tx - hx .. C0 + tx - 1
+    tbs = zstride4(tx + g["xpw"])
+    assert (tx - w) + g["xpw"] + w <= tbs and g["C0"] + g["hx"] <= tbs
+    assert g["C0"] + tx - g["hx"] >= 0 and g["C0"] + tx - 1 < tbs
+    if (nx, nz, px) == (256, 200, 65):
+        assert max(smem.values()) <= 232448, smem
