@@ -1,6 +1,7 @@
 // bulk_copy.cuh -- shared-memory staging with the bulk-copy (TMA) engine:
-// one-dimensional cp.async.bulk global -> shared copies (no multicast) that
-// complete on an mbarrier, and a bounded wait on that mbarrier.
+// one-dimensional cp.async.bulk global -> shared copies into the issuing
+// block's own shared memory that complete on an mbarrier, and a bounded wait
+// on that mbarrier.
 #pragma once
 #include <cuda_runtime.h>
 
