@@ -290,6 +290,12 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     S = GE.load_package()
     L = S._native.lib()
+    if args.study:  # one named study alone: its reconstructions/s, kernel split, rooflines, parity
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # 256 MB > 126 MB L2
+        res = run_study(S, L, torch, args.study, args, peaks(S, L), flush)
+        if rank == 0:
+            print(json.dumps({"study": args.study, "unit": "recons/s", "higher_is_better": True, **res}), flush=True)
+        return
     st = build_study(S, lambda s: S.SPECTplan(s.mumap, s.psfs, s.dy))
     plan = S.SPECTplan(st.mumap, st.psfs, st.dy)
     nx, ny, nz = plan.imgsize
@@ -858,6 +864,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the batched/served measurements")
     ap.add_argument("--served-jobs", type=int, default=500)
     ap.add_argument("--served-rate", type=float, default=10.0)
+    ap.add_argument("--study", choices=["small_64x64x64", "large_256x256x200"],
+                    help="run only this study (the small 64^3 ML-EM or the large 256x256x200 OS-EM) and print its line")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
