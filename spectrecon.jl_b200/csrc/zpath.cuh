@@ -26,10 +26,12 @@
 // k_zadj   backproject! (src/backproject.jl:69-124), convolution half: per
 //          plane the x pass and z pass of fft_conv_adj! (src/fft_convolve.jl:
 //          82-130) of the view, times the attenuation, stored as T.
+// The kernels for planes too large for these kernels' shared memory are in
+// zstrip.cuh (same layouts and passes, over plane tiles).
 // k_zrot_adj  imrotate_adj! :two (src/rotatez.jl:390-416) and the view sum
-//          (src/backproject.jl:146-153): output-stationary gather.  A group of
-//          8 lanes owns one image column (x, y) over all z (8 lanes x ZPL) and
-//          sums, over the group's views in order, the bilinear weights of the
+//          (src/backproject.jl:146-153): output-stationary gather.  Groups of
+//          8 lanes own one image column (x, y) over all z (8 lanes x ZPL) and
+//          sum, over their views in order, the bilinear weights of the
 //          rotated-grid points whose footprint covers it: the exact transpose
 //          of the forward sampling, without atomics.  The EM update
 //          (src/ml-os-em.jl:111-126) is its epilogue.
@@ -748,9 +750,11 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 // ------------------------------------------------------------------------
 // k_zrot_adj<ZPL>: two 8-lane groups of a warp own image column p = (j1, j2)
 // (grid-stride), lane l of a group the z pairs 2 l + 16 q, q < ZPL / 2 (nzp =
-// 8 ZPL): 64 contiguous bytes per group and 8-byte load, the candidate
-// geometry shared by the group's 8 lanes.  The first group sums the even slots, the second
-// the odd ones; a shuffle adds the two partial sums (a fixed order).  For
+// 8 ZPL): 64 contiguous bytes per group and 8-byte load.  The first group
+// sums the even slots, the second the odd ones; a shuffle adds the two
+// partial sums (a fixed order).  Per slot, lane l of a group evaluates
+// candidate l (and every lane candidate 8) and the group shares the nine by
+// shuffles, summing them in the order 0..8.  For
 // every slot, the rotated-grid points (x, y) whose bilinear footprint contains
 // (j1, j2) -- those with floor(s1) in {j1-1, j1} and floor(s2) in {j2-1, j2}
 // -- lie within |cos| + |sin| of the inverse-rotated pixel centre, so the
