@@ -240,7 +240,7 @@ struct spect_plan_s {
   // large-plane kernels (zpath == 2): task width, column / row tiles, shared
   // memory and resident blocks per SM of k_zs_fz, k_zs_fx, k_zs_adj, and the
   // forward's plane-tile exchange buffer
-  int zs_w = 8, zs_tx = 8, zs_tz = 4;
+  int zs_w = 8, zs_tx = 8, zs_tz = 4, zs_fz_nth = kZsNth / 2, zs_adj_nth = kZsNth, zs_adj_tx = 8;
   size_t zs_smem[3] = {0, 0, 0};
   int zs_occ[3] = {1, 1, 1};
   float* d_Q = nullptr;
@@ -593,7 +593,7 @@ int zforward(spect_plan_s* p, float* views, const float* imgIZ, const int* vidx,
       a.tz = p->zs_tz;
       const int n1 = nv * p->ny * (p->nx / p->zs_tx), n2 = nv * nc * ntz;
       LAUNCH(p, K_CONV_FWD, st, "k_zs_fz",
-             zs_fz_launch(p->zs_w, std::min(n1, p->sm_count * p->zs_occ[0]), p->zs_smem[0], st, a));
+             zs_fz_launch(p->zs_w, p->zs_fz_nth, std::min(n1, p->sm_count * p->zs_occ[0]), p->zs_smem[0], st, a));
       LAUNCH(p, K_CONV_FWD, st, "k_zs_fx",
              zs_fx_launch(p->zs_w, std::min(n2, p->sm_count * p->zs_occ[1]), p->zs_smem[1], st, a));
     } else {
@@ -632,13 +632,14 @@ int zbackward(spect_plan_s* p, float* outIZ, const float* views, const int* vidx
     a.vidx = vi;
     a.nv = nv;
     if (p->zpath == 2) {  // large planes: column tiles, x pass and z pass x attenuation -> T
-      const int ntx = p->nx / p->zs_tx;
+      const int ntx = p->nx / p->zs_adj_tx;
       zs_chunking(p, nv, ntx, &cy, &nc);
       a.chunkY = cy;
       a.nchunks = nc;
-      a.tx = p->zs_tx;
+      a.tx = p->zs_adj_tx;
       LAUNCH(p, K_CONV_ADJ, st, "k_zs_adj",
-             zs_adj_launch(p->zs_w, std::min(nv * ntx * nc, p->sm_count * p->zs_occ[2]), p->zs_smem[2], st, a));
+             zs_adj_launch(p->zs_w, p->zs_adj_nth, std::min(nv * ntx * nc, p->sm_count * p->zs_occ[2]),
+                           p->zs_smem[2], st, a));
     } else {
       chunking(p, nv, true, &cy, &nc);
       a.chunkY = cy;
@@ -1629,9 +1630,21 @@ int plan_create_impl(spect_plan_t* out, int nx, int ny, int nz, int px, int pz, 
     p->zs_tz = zt.tz;
     p->zs_smem[0] = zs_fz_smem(zg, zt.tx);
     p->zs_smem[1] = zs_fx_smem(zg, zt.tz);
-    p->zs_smem[2] = zs_adj_smem(zg, zt.tx);
+    // k_zs_fz: 256 threads, two blocks per SM (SPECT_ZS_FZ_THREADS=512: one of 512)
+    const char* fz_env = std::getenv("SPECT_ZS_FZ_THREADS");
+    p->zs_fz_nth = (fz_env && std::atoi(fz_env) == kZsNth) ? kZsNth : kZsNth / 2;
+    // k_zs_adj: 512 threads on tiles of tx columns (SPECT_ZS_ADJ_THREADS=256:
+    // 256 threads on tiles of half the width, two blocks per SM where they fit)
+    const char* adj_env = std::getenv("SPECT_ZS_ADJ_THREADS");
+    p->zs_adj_nth = kZsNth;
+    p->zs_adj_tx = zt.tx;
+    if (adj_env && std::atoi(adj_env) == kZsNth / 2 && zt.tx / 2 >= zt.w && zt.tx % 2 == 0 && (zt.tx / 2) % 4 == 0) {
+      p->zs_adj_nth = kZsNth / 2;
+      p->zs_adj_tx = zt.tx / 2;
+    }
+    p->zs_smem[2] = zs_adj_smem(zg, p->zs_adj_tx);
     cudaError_t ze = zstrip_setup((int)p->max_smem);
-    if (ze == cudaSuccess) ze = zstrip_occupancy(zt.w, p->zs_smem, p->zs_occ);
+    if (ze == cudaSuccess) ze = zstrip_occupancy(zt.w, p->zs_fz_nth, p->zs_adj_nth, p->zs_smem, p->zs_occ);
     if (ze != cudaSuccess) return bail(fail(SPECT_ERR_CUDA, std::string("large-plane kernel setup: ") + cudaGetErrorString(ze)));
   }
   if (p->zpath == 1) {

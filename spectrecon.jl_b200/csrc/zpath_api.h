@@ -138,10 +138,10 @@ cudaError_t zfrom_iz_launch(const ZGeom& g, cudaStream_t st, const float* iz, fl
 // SM of k_zs_fz, k_zs_fx, k_zs_adj at their shared-memory sizes (for the
 // persistent grids)
 cudaError_t zstrip_setup(int max_smem);
-cudaError_t zstrip_occupancy(int w, const size_t smem[3], int occ[3]);
-cudaError_t zs_fz_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
+cudaError_t zstrip_occupancy(int w, int fz_nth, int adj_nth, const size_t smem[3], int occ[3]);
+cudaError_t zs_fz_launch(int w, int nth, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
 cudaError_t zs_fx_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
-cudaError_t zs_adj_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
+cudaError_t zs_adj_launch(int w, int nth, int grid, size_t smem, cudaStream_t st, const ZArgs& a);
 cudaError_t zatten_launch(const ZGeom& g, int nview, cudaStream_t st, const float* muz, const float4* rot, float dy,
                           float* att);
 

@@ -61,9 +61,13 @@ cudaError_t zrot_adj_launch(const ZGeom& g, int grid, cudaStream_t st, const flo
 }
 
 namespace {
-const void* const kZsFz[2] = {(const void*)k_zs_fz<kZsNth, 8>, (const void*)k_zs_fz<kZsNth, 16>};
+// k_zs_fz: 512 threads (index 0, 1) or 256 (index 2, 3: two blocks per SM at these registers)
+const void* const kZsFz[4] = {(const void*)k_zs_fz<kZsNth, 8>, (const void*)k_zs_fz<kZsNth, 16>,
+                              (const void*)k_zs_fz<kZsNth / 2, 8>, (const void*)k_zs_fz<kZsNth / 2, 16>};
 const void* const kZsFx[2] = {(const void*)k_zs_fx<kZsNthX, 8>, (const void*)k_zs_fx<kZsNthX, 16>};
-const void* const kZsAdj[2] = {(const void*)k_zs_adj<kZsNth, 8>, (const void*)k_zs_adj<kZsNth, 16>};
+// k_zs_adj: 512 threads (index 0, 1) or 256 (index 2, 3: narrower tiles, two blocks per SM)
+const void* const kZsAdj[4] = {(const void*)k_zs_adj<kZsNth, 8>, (const void*)k_zs_adj<kZsNth, 16>,
+                               (const void*)k_zs_adj<kZsNth / 2, 8>, (const void*)k_zs_adj<kZsNth / 2, 16>};
 cudaError_t zs_launch(const void* k, int nth, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
   ZArgs c = a;
   void* args[] = {&c};
@@ -73,17 +77,17 @@ cudaError_t zs_launch(const void* k, int nth, int grid, size_t smem, cudaStream_
 
 cudaError_t zstrip_setup(int max_smem) {
   for (int i = 0; i < 2; ++i)
-    for (const void* k : {kZsFz[i], kZsFx[i], kZsAdj[i]}) {
+    for (const void* k : {kZsFz[i], kZsFz[i + 2], kZsFx[i], kZsAdj[i], kZsAdj[i + 2]}) {
       const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem);
       if (e != cudaSuccess) return e;
     }
   return cudaSuccess;
 }
 
-cudaError_t zstrip_occupancy(int w, const size_t smem[3], int occ[3]) {
-  const int i = w == 16 ? 1 : 0;
-  const void* ks[3] = {kZsFz[i], kZsFx[i], kZsAdj[i]};
-  const int nth[3] = {kZsNth, kZsNthX, kZsNth};
+cudaError_t zstrip_occupancy(int w, int fz_nth, int adj_nth, const size_t smem[3], int occ[3]) {
+  const int i = w == 16 ? 1 : 0, f = fz_nth == kZsNth ? i : i + 2, d = adj_nth == kZsNth ? i : i + 2;
+  const void* ks[3] = {kZsFz[f], kZsFx[i], kZsAdj[d]};
+  const int nth[3] = {fz_nth, kZsNthX, adj_nth};
   for (int j = 0; j < 3; ++j) {
     const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[j], ks[j], nth[j], smem[j]);
     if (e != cudaSuccess) return e;
@@ -92,14 +96,14 @@ cudaError_t zstrip_occupancy(int w, const size_t smem[3], int occ[3]) {
   return cudaSuccess;
 }
 
-cudaError_t zs_fz_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
-  return zs_launch(kZsFz[w == 16 ? 1 : 0], kZsNth, grid, smem, st, a);
+cudaError_t zs_fz_launch(int w, int nth, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
+  return zs_launch(kZsFz[(w == 16 ? 1 : 0) + (nth == kZsNth ? 0 : 2)], nth, grid, smem, st, a);
 }
 cudaError_t zs_fx_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
   return zs_launch(kZsFx[w == 16 ? 1 : 0], kZsNthX, grid, smem, st, a);
 }
-cudaError_t zs_adj_launch(int w, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
-  return zs_launch(kZsAdj[w == 16 ? 1 : 0], kZsNth, grid, smem, st, a);
+cudaError_t zs_adj_launch(int w, int nth, int grid, size_t smem, cudaStream_t st, const ZArgs& a) {
+  return zs_launch(kZsAdj[(w == 16 ? 1 : 0) + (nth == kZsNth ? 0 : 2)], nth, grid, smem, st, a);
 }
 
 cudaError_t zto_iz_launch(const ZGeom& g, cudaStream_t st, const float* img, float* iz) {
