@@ -385,7 +385,7 @@ def run_ours(args):
     pk = peaks(S, L)
     split, roofs = kernel_table(plan, kms, kn, args.steps, nsub, pk)
     dom = dict(roofs[0]) if roofs else {}
-    traffic = read_traffic(f"{dom.get('kernel')}_c2.md") if dom else None
+    traffic = read_traffic(f"{dom.get('kernel')}_128x128x80.md") if dom else None
     roofline = dict(dom, traffic=traffic, traffic_source="ncu dram bytes per launch (profiles/)" if traffic else None,
                     peak_source=pk["fp32_source"] if dom.get("bound") == "fp32" else pk["hbm_source"])
     batched = served = None

@@ -71,7 +71,7 @@ def test_large_512_planes(S, O, monkeypatch, path):
     assert relerr(b, b64) <= TOL
     assert relerr(b, b32) <= max(TOL, 1.5 * relerr(b32, b64))
 
-def test_full_c2_subset_osem_update(S, O):
+def test_full_128x128x80_subset_osem_update(S, O):
     """One OS-EM iteration (8 subsets of 15 views) of the benchmark study vs the oracle."""
     import importlib
     W = importlib.import_module("spectrecon_b200.workloads")
