@@ -67,6 +67,16 @@ namespace spect {
 
 __device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void st4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+// 8-byte read-only global load issued only where pred holds; (0, 0) elsewhere
+// (no memory access for those lanes).  p must be 8-byte aligned.
+__device__ __forceinline__ float2 ldg2_if(const float* p, bool pred) {
+  unsigned a, b;
+  asm("{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %3, 0;\n\tmov.b32 %0, 0;\n\tmov.b32 %1, 0;\n\t"
+      "@q ld.global.nc.v2.b32 {%0, %1}, [%2];\n\t}"
+      : "=r"(a), "=r"(b)
+      : "l"(p), "r"((int)pred));
+  return make_float2(__uint_as_float(a), __uint_as_float(b));
+}
 
 // one W-output task (W = 8 or 16) over a zero-padded line, the taps
 // m in [4 b4, 4 b4 + 8 nblk) in blocks of 8 (nblk <= 9): o[k] += sum_m w[m]
@@ -760,9 +770,15 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 // -- lie within |cos| + |sin| of the inverse-rotated pixel centre, so the
 // candidates are at most 3 x 3 points; each is tested with the forward's own
 // position arithmetic and weighted with the forward's weight product.
+// RB = 0: a hit candidate's loads are issued under a branch on its offset,
+// so the candidates' load latencies follow one another.  RB > 0: the
+// candidates go in rounds of RB whose loads are all issued (predicated off
+// for misses, which then read zero) before the round's FMAs, so up to
+// RB x ZPL / 2 loads per lane are in flight; a miss adds fmaf(0, 0, acc) ==
+// acc, so both forms give the same bits.
 // Epilogue (IZ layout): v = acc (+ prev); mode 1: zeros -> +Inf; mode 2:
 // v = x * (v / asum); out = v (z < nz only; out may be prev or x).
-template <int ZPL>
+template <int ZPL, int RB>
 __global__ void __launch_bounds__(256, (ZPL <= 14 ? 4 : 2)) k_zrot_adj(ZGeom g, const float* __restrict__ T,
                                                  const float4* __restrict__ rot, const int* __restrict__ vidx, int nv,
                                                  const float* prev, float* out, const float* x,
@@ -815,17 +831,47 @@ __global__ void __launch_bounds__(256, (ZPL <= 14 ? 4 : 2)) k_zrot_adj(ZGeom g, 
       int ol, o8;
       cand(lane, wl, ol);
       cand(8, w8, o8);
+      if constexpr (RB == 0) {
 #pragma unroll
-      for (int c = 0; c < 9; ++c) {
-        const float w = c < 8 ? __shfl_sync(0xffffffffu, wl, c, 8) : w8;
-        const int o = c < 8 ? __shfl_sync(0xffffffffu, ol, c, 8) : o8;
-        if (o >= 0) {
-          const float* tp = Ts + o;
+        for (int c = 0; c < 9; ++c) {
+          const float w = c < 8 ? __shfl_sync(0xffffffffu, wl, c, 8) : w8;
+          const int o = c < 8 ? __shfl_sync(0xffffffffu, ol, c, 8) : o8;
+          if (o >= 0) {
+            const float* tp = Ts + o;
 #pragma unroll
-          for (int q = 0; q < ZPL / 2; ++q) {
-            const float2 t = *reinterpret_cast<const float2*>(tp + 16 * q);
-            acc[q].x = fmaf(w, t.x, acc[q].x);
-            acc[q].y = fmaf(w, t.y, acc[q].y);
+            for (int q = 0; q < ZPL / 2; ++q) {
+              const float2 t = *reinterpret_cast<const float2*>(tp + 16 * q);
+              acc[q].x = fmaf(w, t.x, acc[q].x);
+              acc[q].y = fmaf(w, t.y, acc[q].y);
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int c0 = 0; c0 < 9; c0 += RB) {
+          float wk[RB];
+          float2 tk[RB][ZPL / 2];
+#pragma unroll
+          for (int k = 0; k < RB; ++k) {
+            const int c = c0 + k;
+            wk[k] = 0.f;
+            if (c < 9) {  // resolved at compile time
+              wk[k] = c < 8 ? __shfl_sync(0xffffffffu, wl, c, 8) : w8;
+              const int o = c < 8 ? __shfl_sync(0xffffffffu, ol, c, 8) : o8;
+              const float* tp = Ts + max(o, 0);
+#pragma unroll
+              for (int q = 0; q < ZPL / 2; ++q) tk[k][q] = ldg2_if(tp + 16 * q, o >= 0);
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < RB; ++k) {
+            if (c0 + k < 9) {
+#pragma unroll
+              for (int q = 0; q < ZPL / 2; ++q) {
+                acc[q].x = fmaf(wk[k], tk[k][q].x, acc[q].x);
+                acc[q].y = fmaf(wk[k], tk[k][q].y, acc[q].y);
+              }
+            }
           }
         }
       }

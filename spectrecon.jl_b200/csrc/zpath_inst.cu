@@ -1,6 +1,8 @@
 // zpath_inst.cu -- instantiations and launchers of the fused projector pair
 // (zpath.cuh) and of the large-plane kernels (zstrip.cuh), compiled as a unit
 // of its own.
+#include <cstdlib>
+
 #include "zpath.cuh"
 #include "zstrip.cuh"
 
@@ -18,10 +20,29 @@ const void* const kZfwd[kZNShapes] = ZSHAPES(k_zfwd);
 const void* const kZadj[kZNShapes] = ZSHAPES(k_zadj);
 #undef ZSHAPES
 
+// k_zrot_adj's candidates per load round: the largest of 3 and 2 whose
+// rounds compile without register spills under the kernel's launch bounds
+// (64 registers per thread for ZPL <= 14, 128 above; from ptxas -v for
+// every ZPL); 0 (one branch per candidate) where both spill.
+// SPECT_ZROT_RB=0 selects the branch form everywhere; read once per process.
+constexpr int zrot_rounds(int zpl) {
+  return (zpl <= 10 || (zpl >= 16 && zpl <= 24)) ? 3 : (zpl == 26 || zpl >= 30) ? 2 : 0;
+}
+bool zrot_branch_form() {
+  static const bool b = [] {
+    const char* e = getenv("SPECT_ZROT_RB");
+    return e != nullptr && e[0] == '0' && e[1] == 0;
+  }();
+  return b;
+}
+
 template <int ZPL>
 cudaError_t zrot(const ZGeom& g, int grid, cudaStream_t st, const float* T, const float4* rot, const int* vidx,
                  int nv, const float* prev, float* out, const float* x, const float* asum, int mode) {
-  k_zrot_adj<ZPL><<<grid, 256, 0, st>>>(g, T, rot, vidx, nv, prev, out, x, asum, mode);
+  if (zrot_branch_form())
+    k_zrot_adj<ZPL, 0><<<grid, 256, 0, st>>>(g, T, rot, vidx, nv, prev, out, x, asum, mode);
+  else
+    k_zrot_adj<ZPL, zrot_rounds(ZPL)><<<grid, 256, 0, st>>>(g, T, rot, vidx, nv, prev, out, x, asum, mode);
   return cudaGetLastError();
 }
 }  // namespace
