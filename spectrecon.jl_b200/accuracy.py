@@ -1,4 +1,4 @@
-"""Accuracy harness over MATLAB data files (accuracy/project.jl:1-62).
+"""Accuracy harness over MATLAB data files (accuracy/project.jl:1-60).
 
 The reference's accuracy script reads four ``.mat`` files made with the MIRT
 MATLAB toolbox -- ``mumap208.mat`` (variable ``mumap208``), ``psf_208.mat``
@@ -99,7 +99,7 @@ def load_project_data(path):
 
 def project_error(path="../data/", interpmeths=("one", "two"), modes=("fast", "mem"), dy=PROJECT_DY,
                   data=None, verbose=True):
-    """accuracy/project.jl:18-59: for every interpolation method and mode,
+    """accuracy/project.jl:18-55: for every interpolation method and mode,
     project ``xtrue`` through a plan of ``mumap`` and ``psfs`` on the GPU and
     return ``{(interpmeth, mode): nrmse}`` against the supplied projections.
 

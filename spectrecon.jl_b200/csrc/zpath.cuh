@@ -758,7 +758,7 @@ __global__ void __launch_bounds__(NTH, 1) k_zadj(ZArgs a) {
 }
 
 // ------------------------------------------------------------------------
-// k_zrot_adj<ZPL>: two 8-lane groups of a warp own image column p = (j1, j2)
+// k_zrot_adj<ZPL, RB>: two 8-lane groups of a warp own image column p = (j1, j2)
 // (grid-stride), lane l of a group the z pairs 2 l + 16 q, q < ZPL / 2 (nzp =
 // 8 ZPL): 64 contiguous bytes per group and 8-byte load.  The first group
 // sums the even slots, the second the odd ones; a shuffle adds the two

@@ -65,7 +65,7 @@ def test_rot90_family(O, m, np_k):  # test/rotatez.jl:7-46 (rotl90/rot180/rotr90
     assert np.array_equal(O.rot_f90(O.rot_f90(A, m), m, adj=True), A)
 
 
-def test_rot_f90_invalid(O):  # test/rotatez.jl:198-207
+def test_rot_f90_invalid(O):  # src/rotatez.jl:197-210 (m outside 0..3 throws)
     A = np.zeros((20, 20), np.float32)
     for m in (-1, 4):
         with pytest.raises(ValueError):
@@ -84,7 +84,7 @@ def test_rotate_bounds(O, method):  # test/adjoint-rotate.jl:28-46
 
 
 @pytest.mark.parametrize("method", ["one", "two"])
-def test_rotate_adjoint_matrix(O, method):  # test/adjoint-rotate.jl:50-66
+def test_rotate_adjoint_matrix(O, method):  # test/adjoint-rotate.jl:43-59
     M = 16
     for k in range(7):
         th = np.float32(k / 7 * 2 * np.pi)
