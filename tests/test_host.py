@@ -131,3 +131,59 @@ def test_replica_aggregation_gloo():
                          env=env, capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr[-2000:]
     assert out.stdout.count("ok") == 2
+
+
+_C_CALLER = r"""
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include "spect_gpu.h"
+
+int main(void) {
+  enum { NY = 4, PX = 5, PZ = 3 };
+  float psf[NY * PZ * PX];
+  double fx[NY] = {0.0, 1.0, 2.0, 3.0}, fz[NY] = {0.0, 1.5, 1.5, 2.5};
+  float mumap[8 * 6 * 4] = {0}, psfs[3 * 3 * 6 * 2];
+  spect_plan_t plan = NULL;
+  int y, i, rc;
+  if (spect_psf_gauss(psf, NY, PX, PZ, fx, fz) != SPECT_OK) return 1;
+  for (y = 0; y < NY; ++y) {
+    double s = 0.0;
+    for (i = 0; i < PX * PZ; ++i) s += psf[y * PX * PZ + i];
+    if (fabs(s - 1.0) > 1e-6) return 2;
+  }
+  /* fwhm 0 on both axes: the impulse at the centre (test/psf-gauss.jl) */
+  if (psf[(PZ / 2) * PX + PX / 2] != 1.0f) return 3;
+  for (i = 0; i < 3 * 3 * 6 * 2; ++i) psfs[i] = 1.0f / 9.0f;
+  /* nx = 8 != ny = 6: the reference's throw string, no device needed */
+  rc = spect_plan_create(&plan, 8, 6, 4, 3, 3, 2, mumap, psfs, 4.8f, NULL, SPECT_INTERP_TWO,
+                         SPECT_MODE_FAST, 1, 1);
+  if (rc != SPECT_ERR_NX_NE_NY || strstr(spect_last_error(), "nx != ny") == NULL) return 4;
+  if (spect_psf_gauss(NULL, NY, PX, PZ, fx, fz) == SPECT_OK) return 5;
+  printf("ok\n");
+  return 0;
+}
+"""
+
+
+def test_c_caller_compiles_and_runs(S, tmp_path):
+    """A C99 caller of include/spect_gpu.h (the boundary that Julia's ccall
+    and C hosts bind) compiles without warnings, links libspectgpu.so and
+    gets the host generator's results and the reference's error text
+    without touching a device."""
+    import shutil
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lib = os.path.join(ROOT, "spectrecon.jl_b200", "libspectgpu.so")
+    S._native.lib()  # builds the library when missing
+    src = tmp_path / "caller.c"
+    src.write_text(_C_CALLER)
+    exe = tmp_path / "caller"
+    cmd = [cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+           str(src), "-o", str(exe), lib, f"-Wl,-rpath,{os.path.dirname(lib)}", "-lm"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    assert out.stdout.strip() == "ok"
